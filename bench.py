@@ -1,0 +1,380 @@
+"""Benchmark of the adaptive cubature hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload oscillatory_cornerpeak_8d | gaussian_5d | productpeak_6d_batch]
+
+A step integrates one batch of the workload to its epsrel through the
+library's public C ABI (cub_integrate / cub_integrate_batch).  The default
+workload is the 8-D Genz pair: oscillatory cos(2 pi 0.3 + sum 1.1 x_i) and
+corner peak (1 + sum 0.5 x_i)^-9 on [0,1]^8, FP64, epsrel 1e-6, epsabs 1e-12
+(synthetic parameters as specified; the analytic integral checks every
+result).  Metric: integrals/s (whole job, all GPUs), with Geval/s beside it.
+
+--impl reference times the reference algorithm's CPU implementation (the
+oracle port of the two-phase engine, oracle/cuhre_oracle.c) on the host
+cores with all threads, on the same workload.
+
+Under torchrun each rank runs its own replica of the workload on its GPU
+(the path does not shard a single integral); steps are bracketed by a
+barrier and device synchronisation, and the max time over ranks is used.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "old-gpuintegration_b200"))
+sys.path.insert(0, str(ROOT / "oracle"))
+
+WORKLOADS = {
+    # name: (family list, ndim, a, u, epsrel, epsabs, batch)
+    "oscillatory_cornerpeak_8d": {
+        "items": [("oscillatory", 8, 1.1, 0.3), ("corner_peak", 8, 0.5, 0.0)],
+        "epsrel": 1e-6, "epsabs": 1e-12,
+    },
+    "gaussian_5d": {
+        "items": [("gaussian", 5, 5.0, 0.5)], "epsrel": 1e-3, "epsabs": 1e-12,
+    },
+    "productpeak_6d_batch": {
+        "batch": ("product_peak", 6, 4096), "epsrel": 1e-5, "epsabs": 1e-12,
+    },
+}
+
+# Algorithmic FP64 flops per integrand evaluation, FMA = 2 (transcendental
+# calls counted separately): map 2n + 5 rule FMAs 10 + Jacobian 1 + f.
+F_FAMILY = {
+    "gaussian": lambda n: 4 * n + 1,
+    "oscillatory": lambda n: 2 * n + 2,
+    "corner_peak": lambda n: 2 * n + 1 + 4 + 1,
+    "product_peak": lambda n: 5 * n + (n - 1) + 1,
+}
+
+
+def flops_per_region(family: str, n: int) -> float:
+    from cubature import npoints
+
+    per_eval = 2 * n + 10 + 1 + F_FAMILY[family](n)
+    return npoints(n) * per_eval + 5 * n + 3 * 9 * 3 + 8
+
+
+def product_peak_params(n: int, count: int):
+    import numpy as np
+
+    out = []
+    for k in range(count):
+        rng = np.random.default_rng(k)
+        a = np.exp(rng.uniform(math.log(1.0), math.log(50.0), n))
+        u = rng.uniform(0.1, 0.9, n)
+        out.append((list(a), list(u)))
+    return out
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.idx = device_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def measure_fp64_peak(torch) -> float:
+    """FP64 dense throughput of cuBLAS DGEMM on this GPU (TFLOP/s), the
+    denominator for the FP64-bound rule kernel."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = float("inf")
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        torch.cuda.synchronize()
+        best = min(best, s.elapsed_time(e) / 1e3)
+    del a, b
+    torch.cuda.empty_cache()
+    return 2 * n ** 3 / best / 1e12
+
+
+def cpu_reference_rate(workload: dict, seconds: float, threads: int = 0):
+    """Integrals/s of the oracle's two-phase engine on the host cores over a
+    bounded sample of the workload (whole integrals, repeated)."""
+    import oracle as O
+
+    jobs = []
+    if "items" in workload:
+        for fam, n, a, u in workload["items"]:
+            jobs.append((fam, n, a, u))
+    else:
+        fam, n, count = workload["batch"]
+        for a, u in product_peak_params(n, count):
+            jobs.append((fam, n, a, u))
+    rules = {}
+    t0 = time.perf_counter()
+    done = 0
+    evals = 0
+    i = 0
+    while True:
+        fam, n, a, u = jobs[i % len(jobs)]
+        R = rules.setdefault(n, O.Rule(n))
+        r = R.integrate_reference(O.make_integrand(fam, n, a, u), workload["epsrel"],
+                                  workload["epsabs"], nthreads=threads)
+        done += 1
+        evals += r["neval"]
+        i += 1
+        el = time.perf_counter() - t0
+        if el >= seconds and done >= len(jobs) if "items" in workload else el >= seconds:
+            break
+    cores = threads if threads > 0 else O.max_threads()
+    return done / el, evals / el, cores, done, el
+
+
+def run_reference(args, workload, world, rank):
+    """The reference arm: CPU implementation of the path on the host cores."""
+    if rank != 0:
+        return 0
+    per_step = max(1.0, 30.0 / max(1, args.steps + args.warmup))
+    for _ in range(args.warmup):
+        cpu_reference_rate(workload, per_step * 0.25)
+    rates, evr = [], []
+    for _ in range(args.steps):
+        r, e, cores, done, el = cpu_reference_rate(workload, per_step)
+        rates.append(r)
+        evr.append(e)
+    value = statistics.median(rates)
+    line = {
+        "impl": "reference", "metric": "integrals/s", "value": value, "unit": "integrals/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 / value, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "epsrel": workload["epsrel"]},
+        "geval_per_s": statistics.median(evr) / 1e9,
+        "cpu_baseline": {"value": value, "unit": "integrals/s", "cores": cores, "kind": "port",
+                         "sample": f"whole integrals of the workload repeated for ~{per_step:.0f} s per step"},
+        "e2e": {"value": value, "unit": "integrals/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="oscillatory_cornerpeak_8d")
+    ap.add_argument("--cpu-seconds", type=float, default=8.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    workload = WORKLOADS[args.workload]
+    world, rank, local = dist_setup()
+
+    if args.impl == "reference":
+        return run_reference(args, workload, world, rank)
+
+    import torch
+    import cubature as cub
+
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+        pg = dist
+
+    ctx = cub.Context(local)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=f"cuda:{local}")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    # the step: integrate the workload through the public C ABI
+    if "items" in workload:
+        items = [cub.Integrand(f, n, a, u) for f, n, a, u in workload["items"]]
+
+        def step():
+            return [ctx.integrate(f, workload["epsrel"], workload["epsabs"]) for f in items]
+
+        fams = [(f.family, f.ndim) for f in items]
+        exact = []
+        import oracle as O
+
+        for f in items:
+            exact.append(O.exact(O.make_integrand(f.family, f.ndim, f.a, f.u)))
+    else:
+        fam, n, count = workload["batch"]
+        plist = [cub.make_params(n, a, u) for a, u in product_peak_params(n, count)]
+
+        def step():
+            return ctx.integrate_batch(fam, n, plist, workload["epsrel"], workload["epsabs"])
+
+        fams = [(fam, n)] * count
+        import oracle as O
+
+        exact = [O.exact(O.make_integrand(fam, n, a, u)) for a, u in product_peak_params(n, count)]
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    ctx.reset_stats()
+    ctx.set_timing(True)
+    step_ms, wall_ms = [], []
+    results = None
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            if pg:
+                pg.barrier()
+            ev0 = torch.cuda.Event(enable_timing=True)
+            ev1 = torch.cuda.Event(enable_timing=True)
+            ev0.record(stream)
+            t0 = time.perf_counter()
+            results = step()
+            t1 = time.perf_counter()
+            ev1.record(stream)
+            torch.cuda.synchronize()
+            step_ms.append(ev0.elapsed_time(ev1))
+            wall_ms.append((t1 - t0) * 1e3)
+    ctx.set_timing(False)
+    st = ctx.stats()
+
+    # correctness of the last step against the analytic integrals
+    nint = len(results)
+    bad = 0
+    for r, ex in zip(results, exact):
+        if not (r.status == 0 and abs(r.integral - ex) <= 2 * workload["epsrel"] * abs(ex)):
+            bad += 1
+    neval = sum(r.neval for r in results)
+    nreg = {}
+    for (fam, n), r in zip(fams, results):
+        nreg[(fam, n)] = nreg.get((fam, n), 0) + r.nregions
+
+    dev_ms = sum(step_ms)
+    wall = sum(wall_ms)
+    if pg:
+        t = torch.tensor([dev_ms, wall], dtype=torch.float64, device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        dev_ms, wall = float(t[0]), float(t[1])
+    value = world * nint * args.steps / (dev_ms / 1e3)
+    e2e_value = world * nint * args.steps / (wall / 1e3)
+
+    # roofline of the rule kernel (FP64-bound)
+    alg_flops = sum(flops_per_region(f, n) * c for (f, n), c in nreg.items()) * args.steps
+    achieved = alg_flops / (st["ms_eval"] / 1e3) / 1e12 if st["ms_eval"] > 0 else None
+    peak = measure_fp64_peak(torch) if rank == 0 else None
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        rate, evr, cores, done, el = cpu_reference_rate(workload, args.cpu_seconds)
+        cpu = {"value": rate, "unit": "integrals/s", "cores": cores, "kind": "port",
+               "sample": f"{done} whole integrals of the workload in {el:.1f} s "
+                         "(oracle two-phase engine, OpenMP over regions)"}
+
+    if rank == 0:
+        line = {
+            "metric": "integrals/s", "value": value, "unit": "integrals/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": args.workload, "integrals_per_step": nint,
+                       "epsrel": workload["epsrel"], "epsabs": workload["epsabs"],
+                       "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "flushed between steps (256 MB write)",
+                       "regions_per_step": int(sum(nreg.values()))},
+            "geval_per_s": world * neval * args.steps / (dev_ms / 1e3) / 1e9,
+            "e2e": {"value": e2e_value, "unit": "integrals/s",
+                    "h2d_bytes_per_step": st.get("h2d_bytes", 0) // max(1, args.steps),
+                    "d2h_bytes_per_step": st.get("d2h_bytes", 0) // max(1, args.steps)},
+            "gpu_launches": st["launches"],
+            "roofline": {"kernel": "k_eval (rule)", "bound": "fp64", "achieved": achieved,
+                         "peak": peak, "unit": "TFLOP/s",
+                         "frac": (achieved / peak) if achieved and peak else None,
+                         "traffic": None,
+                         "peak_source": "in-run cuBLAS DGEMM 8192^3 (MEASURED_PEAKS.json has no FP64 figure)",
+                         "eval_ms_per_step": st["ms_eval"] / args.steps,
+                         "eval_launches_per_step": st["eval_launches"] / args.steps},
+            "cpu_baseline": cpu,
+            "clocks": clocks.summary(),
+            "check": {"integrals": nint, "failed": bad},
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0 if bad == 0 else 3
+
+
+if __name__ == "__main__":
+    sys.exit(main())

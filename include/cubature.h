@@ -1,0 +1,200 @@
+/*
+ * cubature.h -- C ABI of the B200 adaptive cubature engine.
+ *
+ * The reference engine (marcpaterno/old-gpuintegration) is a header-only
+ * C++ template, quad::GPUcuhre<T>, with one entry point:
+ *
+ *   GPUcuhre(int argc, char** argv, int dim, int key = 0, int verbose = 0,
+ *            int numDevices = 1)                     quad/GPUquad/GPUquad.h:46-63
+ *   template <class F> int integrate(T epsrel, T epsabs, T& integral,
+ *            T& error, size_t& nregions, size_t& neval, F* f,
+ *            Volume* vol = NULL)                      quad/GPUquad/GPUquad.h:611-727
+ *
+ * This ABI is what a foreign-language binding of that path binds: plain
+ * pointers and sizes, no C++ or torch types.  Built-in integrand families
+ * are selected by id with a parameter block (arbitrary device functors go
+ * through the C++ template front end, include/cubature/gpucuhre.cuh).
+ *
+ * Error handling: every function returns an int; negative values are API or
+ * CUDA errors (message in cub_last_error()), positive values are numerical
+ * statuses.  Nothing calls exit(), resets a device or uses device malloc.
+ *
+ * Threading: one cub_ctx per host thread (a context owns its stream and
+ * its device pools); distinct contexts may be used concurrently.
+ */
+#ifndef CUBATURE_H
+#define CUBATURE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CUB_MAXDIM 16
+#define CUB_MIN_NDIM 2
+#define CUB_MAX_NDIM 8 /* dimensions instantiated in the prebuilt library */
+
+/* Integrand families (Genz test families + the reference driver's own). */
+enum cub_family {
+  CUB_GAUSSIAN = 1,      /* exp(-sum a_i^2 (x_i-u_i)^2)                    */
+  CUB_OSCILLATORY = 2,   /* cos(2 pi u_0 + sum a_i x_i)                    */
+  CUB_CORNER_PEAK = 3,   /* (1 + sum a_i x_i)^-(n+1)                       */
+  CUB_PRODUCT_PEAK = 4,  /* prod 1/(a_i^-2 + (x_i-u_i)^2)                  */
+  CUB_CONTINUOUS = 5,    /* exp(-sum a_i |x_i-u_i|)                        */
+  CUB_DISCONTINUOUS = 6, /* 0 if x_0>u_0 or x_1>u_1, else exp(sum a_i x_i) */
+  CUB_COSSUM = 7         /* -sum cos(10 x_i)/0.054402111088937/2
+                            (reference cudaCuhre.cu:9-23)                  */
+};
+
+/* Region classification / phase structure. */
+enum cub_policy {
+  /* The reference's two phases: breadth-first until 2^14 children or 100
+   * iterations, then each leftover box refined depth-first with its own
+   * tolerance and at most 2048 bisections (GPUKernelquad.cu:609-911). */
+  CUB_POLICY_REFERENCE = 0,
+  /* Breadth-first only, with the reference's per-region classification,
+   * until convergence or the region capacity. */
+  CUB_POLICY_BREADTH = 1
+};
+
+/* Result status values (cub_result.status). */
+#define CUB_STATUS_OK 0 /* converged (reference errorFlag == 0)         */
+/* > 0: not converged; for the reference policy the number of failed
+ * phase-2 boxes (GPUKernelquad.cu:891,910), for the breadth policy 1.  */
+
+/* Error codes (negative return values). */
+#define CUB_ERR_INVALID -1
+#define CUB_ERR_CUDA -2
+#define CUB_ERR_CAPACITY -3
+#define CUB_ERR_UNSUPPORTED -4
+
+typedef struct cub_ctx cub_ctx;
+
+typedef struct cub_genz_params {
+  double a[CUB_MAXDIM]; /* per-axis parameters a_i */
+  double u[CUB_MAXDIM]; /* per-axis offsets u_i    */
+} cub_genz_params;
+
+typedef struct cub_result {
+  double value;                 /* integral estimate                       */
+  double error;                 /* error estimate                          */
+  unsigned long long nregions;  /* regions evaluated (GPUKernelquad.cu:558,884) */
+  unsigned long long neval;     /* integrand evaluations (:559,887-888)    */
+  int status;                   /* CUB_STATUS_OK or > 0                    */
+  int iterations;               /* breadth-first iterations                */
+  int state;                    /* 1 done, 3 stopped at capacity           */
+  int reserved;
+} cub_result;
+
+typedef struct cub_options {
+  int policy;              /* enum cub_policy                              */
+  int phase1_cap;          /* children that end phase 1 (default 16384)    */
+  int max_iters;           /* breadth-first iteration limit (default 100)  */
+  int phase2_max_regions;  /* bisections per leftover box (default 2048)   */
+  long long max_slots;     /* region-list capacity (default 2^26)          */
+  int lanes;               /* lanes per region in the rule kernel; 0 auto  */
+  int reserved;
+} cub_options;
+
+/* Library version, (major << 16) | minor. */
+int cub_version(void);
+
+/* Message of the last error on this host thread ("" if none). */
+const char* cub_last_error(void);
+
+/* Fill *opt with the reference's defaults. */
+void cub_default_options(cub_options* opt);
+
+/* Context on a CUDA device: owns a stream and device pools, grown on demand
+ * and reused across calls.  Replaces the GPUcuhre constructor
+ * (GPUquad.h:46-63), which resets every visible device and parses argv.
+ * Returns NULL on failure. */
+cub_ctx* cub_create(int device);
+void cub_destroy(cub_ctx* ctx);
+
+/* Device bytes currently held by the context's pools. */
+size_t cub_ctx_bytes(const cub_ctx* ctx);
+
+/* The context's CUDA stream (a cudaStream_t), for callers that order their
+ * own work or events against the engine's. */
+void* cub_ctx_stream(cub_ctx* ctx);
+
+/* Counters of the work a context launched since the last reset.  With
+ * timing on, CUDA events bracket every rule-kernel and phase-2 launch and
+ * their device times are summed (adds one event pair per launch). */
+typedef struct cub_stats {
+  double ms_eval;             /* device time of the rule kernel (timing on) */
+  double ms_phase2;           /* device time of the phase-2 kernel          */
+  long long eval_launches;    /* rule-kernel launches                       */
+  long long launches;         /* all kernel launches                        */
+  long long regions_evaluated;/* regions through the rule kernel           */
+  long long iterations;       /* breadth-first iterations                   */
+  long long phase2_boxes;     /* leftover boxes refined depth-first         */
+  long long h2d_bytes;        /* host-to-device bytes copied                */
+  long long d2h_bytes;        /* device-to-host bytes copied                */
+} cub_stats;
+
+int cub_ctx_stats(const cub_ctx* ctx, cub_stats* out);
+void cub_ctx_reset_stats(cub_ctx* ctx);
+void cub_ctx_set_timing(cub_ctx* ctx, int on);
+
+/* One integral over [0,1]^ndim: the body of GPUcuhre::integrate
+ * (GPUquad.h:611-727) for a built-in family.  Unlike the reference, results
+ * are written (not accumulated with +=) into *out.  Returns 0, or a
+ * negative error code; the numerical status is out->status. */
+int cub_integrate(cub_ctx* ctx, int family, int ndim, const cub_genz_params* params,
+                  double epsrel, double epsabs, const cub_options* opt, cub_result* out);
+
+/* `count` independent integrals of one family and dimension, integrated
+ * together (one shared region list).  params/epsrel/epsabs/out have
+ * `count` entries; epsrel/epsabs may be NULL to use epsrel0/epsabs0.  The
+ * reference has no batched form; it would loop over integrate(). */
+int cub_integrate_batch(cub_ctx* ctx, int family, int ndim, int count,
+                        const cub_genz_params* params, const double* epsrel,
+                        const double* epsabs, double epsrel0, double epsabs0,
+                        const cub_options* opt, cub_result* out);
+
+/* ---- per-step entry points on caller device buffers ------------------ */
+
+/* Rule tables of the degree-9 rule for ndim (GPUQuadRule.cu:31-228):
+ * wt/scale/norm are [9][5], count is [9].  Host memory; any may be NULL. */
+int cub_rule_tables(int ndim, double* wt, double* scale, double* norm, int* count);
+
+/* Phase-1 rule + classification over an SoA region list
+ * (INTEGRATE_GPU_PHASE1, GPUQuadPhases.cu:38-79).  Regions are
+ * [lo, lo+len], lo/len laid out [ndim][ld] on the device.  Writes per
+ * region: avg, err, split axis, active (err > max(epsrel|avg|, epsabs)).
+ * params is host memory.  stream may be NULL (default stream). */
+int cub_rule_eval(int family, int ndim, const cub_genz_params* params, long long n,
+                  const double* d_lo, const double* d_len, long long ld, double epsrel,
+                  double epsabs, double* d_avg, double* d_err, int* d_axis, int* d_active,
+                  void* stream);
+
+/* Scratch bytes cub_split / cub_reduce need for n regions. */
+size_t cub_split_scratch_bytes(long long n);
+size_t cub_reduce_scratch_bytes(long long n);
+
+/* Scan + compact + bisect (GenerateActiveIntervals, alignRegions,
+ * divideIntervalsGPU; GPUKernelquad.cu:63-149,357-505).  Every region with
+ * active == 1 yields two children halved on its axis, written [ndim][out_ld]:
+ * layout 0 = the reference's (child 0 of the j-th active region at column j,
+ * child 1 at column m+j); layout 1 = adjacent (2j, 2j+1).  The number of
+ * children 2m is written to *d_count (device).  d_scratch must hold
+ * cub_split_scratch_bytes(n); out_ld must be >= 2m. */
+int cub_split(int ndim, long long n, const double* d_lo, const double* d_len, long long ld,
+              const int* d_active, const int* d_axis, double* d_out_lo, double* d_out_len,
+              long long out_ld, int layout, long long* d_count, void* d_scratch,
+              size_t scratch_bytes, void* stream);
+
+/* The four sums of a phase-1 iteration (GPUKernelquad.cu:565-577):
+ * d_out[0] = sum avg, [1] = sum err, [2] = sum avg over active == 0,
+ * [3] = sum err over active == 0.  Device output; fixed-order tree. */
+int cub_reduce(long long n, const double* d_avg, const double* d_err, const int* d_active,
+               double* d_out, void* d_scratch, size_t scratch_bytes, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CUBATURE_H */

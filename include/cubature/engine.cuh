@@ -1,0 +1,504 @@
+// engine.cuh -- host driver of the breadth-first + depth-first engine.
+//
+// Header-only so user code can integrate its own device functors (the
+// reference's integrate(..., F* f, ...) takes any functor type,
+// quad/GPUquad/GPUquad.h:611-620); the prebuilt library instantiates it for
+// the built-in families.
+//
+// All device memory lives in a Workspace that grows geometrically and is
+// reused across calls (the reference mallocs and frees ~10 buffers per
+// iteration, GPUKernelquad.cu:357-605).  One small pinned D2H copy per
+// iteration tells the host the size of the next region list.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "engine_kernels.cuh"
+#include "phase2_kernels.cuh"
+#include "rule9.hpp"
+
+namespace cubature {
+
+struct Options {
+  int policy = kPolicyReference;  // two-phase reference semantics
+  int phase1_cap = 1 << 14;       // FIRST_PHASE_MAXREGIONS (quad.h:21)
+  int max_iters = 100;            // phase-1 iterations (GPUKernelquad.cu:631)
+  int phase2_max_regions = 2048;  // MAX_GLOBALPOOL_SIZE (quad.h:9)
+  long long max_slots = 1ll << 26;
+  int lanes = 0;                  // lanes per region in eval; 0 = automatic
+};
+
+struct Result {
+  double value, error;
+  unsigned long long nregions, neval;
+  int status;      // reference errorFlag: 0 = converged
+  int iterations;  // phase-1 iterations
+  int state;       // IntegralStateCode at exit
+  int pad;
+};
+
+// Error codes of the host layer (negative; positive values are numerical
+// statuses of individual integrals).
+enum ErrorCode : int {
+  kOk = 0,
+  kErrInvalid = -1,
+  kErrCuda = -2,
+  kErrCapacity = -3,
+};
+
+// Counters of the work a context has launched (reset by the caller).
+struct Stats {
+  double ms_eval = 0;            // summed device time of the rule kernel (timing on)
+  long long eval_launches = 0;   // rule-kernel launches
+  long long launches = 0;        // all kernel launches
+  long long regions_evaluated = 0;
+  long long iterations = 0;      // breadth-first iterations
+  long long phase2_boxes = 0;    // leftover boxes refined depth-first
+  double ms_phase2 = 0;          // device time of the phase-2 kernel (timing on)
+  long long h2d_bytes = 0;       // host-to-device copies issued
+  long long d2h_bytes = 0;       // device-to-host copies issued
+};
+
+inline const char* state_name(int s) {
+  switch (s) {
+    case kStateRunning: return "running";
+    case kStateDone: return "done";
+    case kStatePhase2: return "phase2";
+    case kStateCapacity: return "capacity";
+  }
+  return "?";
+}
+
+class Workspace {
+ public:
+  explicit Workspace(int device = 0) : device_(device) {}
+  ~Workspace() { release(); }
+  Workspace(const Workspace&) = delete;
+  Workspace& operator=(const Workspace&) = delete;
+
+  void release() {
+    for (void*& p : bufs_) {
+      if (p) cudaFree(p);
+      p = nullptr;
+    }
+    if (ctl_host_) cudaFreeHost(ctl_host_);
+    ctl_host_ = nullptr;
+    for (auto& e : ev) {
+      if (e) cudaEventDestroy(e);
+      e = nullptr;
+    }
+    cap_ = left_cap_ = 0;
+    nint_cap_ = 0;
+    slab_bytes_ = 0;
+    ndim_ = 0;
+  }
+
+  int device() const { return device_; }
+  bool timing = false;  // record CUDA events around the rule and phase-2 kernels
+  const std::string& error() const { return err_; }
+  Stats& stats() { return stats_; }
+
+  // Buffers (valid after reserve()).
+  double* lo[2] = {nullptr, nullptr};
+  double* len[2] = {nullptr, nullptr};
+  int* rid[2] = {nullptr, nullptr};
+  double* avg = nullptr;
+  double* err = nullptr;
+  int* axis = nullptr;
+  int* active = nullptr;
+  ChunkPartial* part = nullptr;
+  int* chunk_excl = nullptr;
+  double* left_lo = nullptr;
+  double* left_len = nullptr;
+  int* left_rid = nullptr;
+  LeftoverResult* left_res = nullptr;
+  IntegralState* ist = nullptr;
+  Control* ctl = nullptr;
+  Control* ctl_host_ = nullptr;
+  void* slab = nullptr;
+  int* heap = nullptr;
+  int* counter = nullptr;
+
+  long long cap() const { return cap_; }
+  long long left_cap() const { return left_cap_; }
+
+  // Region lists for `slots` regions of dimension ndim; `cur` survives growth.
+  bool reserve_lists(int ndim, long long slots, int cur, long long keep, cudaStream_t s) {
+    if (slots <= cap_ && ndim == ndim_) return true;
+    long long ncap = std::max<long long>(slots, std::max<long long>(cap_ * 2, 1 << 16));
+    ncap = (ncap + 31) & ~31ll;
+    double *nlo[2] = {nullptr, nullptr}, *nlen[2] = {nullptr, nullptr};
+    int* nrid[2] = {nullptr, nullptr};
+    for (int b = 0; b < 2; ++b) {
+      if (!alloc(&nlo[b], sizeof(double) * ndim * ncap) ||
+          !alloc(&nlen[b], sizeof(double) * ndim * ncap) ||
+          !alloc(&nrid[b], sizeof(int) * ncap))
+        return false;
+    }
+    if (keep > 0 && ndim == ndim_) {
+      for (int d = 0; d < ndim; ++d) {
+        if (!ck(cudaMemcpyAsync(nlo[cur] + d * ncap, lo[cur] + d * cap_, sizeof(double) * keep,
+                                cudaMemcpyDeviceToDevice, s)) ||
+            !ck(cudaMemcpyAsync(nlen[cur] + d * ncap, len[cur] + d * cap_, sizeof(double) * keep,
+                                cudaMemcpyDeviceToDevice, s)))
+          return false;
+      }
+      if (!ck(cudaMemcpyAsync(nrid[cur], rid[cur], sizeof(int) * keep, cudaMemcpyDeviceToDevice, s)))
+        return false;
+      if (!ck(cudaStreamSynchronize(s))) return false;
+    }
+    for (int b = 0; b < 2; ++b) {
+      free_buf(lo[b]);
+      free_buf(len[b]);
+      free_buf(rid[b]);
+      lo[b] = nlo[b];
+      len[b] = nlen[b];
+      rid[b] = nrid[b];
+    }
+    free_buf(avg);
+    free_buf(err);
+    free_buf(axis);
+    free_buf(active);
+    free_buf(part);
+    free_buf(chunk_excl);
+    if (!alloc(&avg, sizeof(double) * ncap) || !alloc(&err, sizeof(double) * ncap) ||
+        !alloc(&axis, sizeof(int) * ncap) || !alloc(&active, sizeof(int) * ncap) ||
+        !alloc(&part, sizeof(ChunkPartial) * (ncap / 32 + 1)) ||
+        !alloc(&chunk_excl, sizeof(int) * (ncap / 32 + 1)))
+      return false;
+    cap_ = ncap;
+    ndim_ = ndim;
+    return true;
+  }
+
+  bool reserve_leftovers(int ndim, long long slots, long long keep, cudaStream_t s) {
+    if (slots <= left_cap_ && ndim == left_ndim_) return true;
+    long long ncap = std::max<long long>(slots, std::max<long long>(left_cap_ * 2, 1 << 14));
+    double *nlo = nullptr, *nlen = nullptr;
+    int* nrid = nullptr;
+    LeftoverResult* nres = nullptr;
+    if (!alloc(&nlo, sizeof(double) * ndim * ncap) || !alloc(&nlen, sizeof(double) * ndim * ncap) ||
+        !alloc(&nrid, sizeof(int) * ncap) || !alloc(&nres, sizeof(LeftoverResult) * ncap))
+      return false;
+    if (keep > 0 && ndim == left_ndim_) {
+      for (int d = 0; d < ndim; ++d) {
+        if (!ck(cudaMemcpyAsync(nlo + d * ncap, left_lo + d * left_cap_, sizeof(double) * keep,
+                                cudaMemcpyDeviceToDevice, s)) ||
+            !ck(cudaMemcpyAsync(nlen + d * ncap, left_len + d * left_cap_, sizeof(double) * keep,
+                                cudaMemcpyDeviceToDevice, s)))
+          return false;
+      }
+      if (!ck(cudaMemcpyAsync(nrid, left_rid, sizeof(int) * keep, cudaMemcpyDeviceToDevice, s)))
+        return false;
+      if (!ck(cudaStreamSynchronize(s))) return false;
+    }
+    free_buf(left_lo);
+    free_buf(left_len);
+    free_buf(left_rid);
+    free_buf(left_res);
+    left_lo = nlo;
+    left_len = nlen;
+    left_rid = nrid;
+    left_res = nres;
+    left_cap_ = ncap;
+    left_ndim_ = ndim;
+    return true;
+  }
+
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+
+  bool reserve_integrals(int nint) {
+    if (!ev[0]) {
+      for (auto& e : ev)
+        if (!ck(cudaEventCreate(&e))) return false;
+    }
+    if (!ctl_host_) {
+      if (!ck(cudaMallocHost(&ctl_host_, sizeof(Control)))) return false;
+      if (!alloc(&ctl, sizeof(Control))) return false;
+      if (!alloc(&counter, sizeof(int) * 4)) return false;
+    }
+    if (nint <= nint_cap_) return true;
+    free_buf(ist);
+    const int n = std::max(nint, 64);
+    if (!alloc(&ist, sizeof(IntegralState) * n)) return false;
+    nint_cap_ = n;
+    return true;
+  }
+
+  bool reserve_slab(size_t bytes, size_t heap_ints) {
+    if (bytes <= slab_bytes_ && heap_ints <= heap_ints_) return true;
+    free_buf(slab);
+    free_buf(heap);
+    if (!alloc(&slab, bytes) || !alloc(&heap, sizeof(int) * heap_ints)) return false;
+    slab_bytes_ = bytes;
+    heap_ints_ = heap_ints;
+    return true;
+  }
+
+  bool ck(cudaError_t e) {
+    if (e != cudaSuccess) {
+      err_ = std::string("CUDA: ") + cudaGetErrorString(e);
+      return false;
+    }
+    return true;
+  }
+
+  size_t bytes_reserved() const { return bytes_; }
+
+ private:
+  template <class T>
+  bool alloc(T** p, size_t bytes) {
+    void* q = nullptr;
+    if (!ck(cudaMalloc(&q, bytes))) return false;
+    *p = static_cast<T*>(q);
+    bufs_.push_back(q);
+    bytes_ += bytes;
+    return true;
+  }
+  template <class T>
+  void free_buf(T*& p) {
+    if (!p) return;
+    for (void*& q : bufs_)
+      if (q == p) {
+        cudaFree(q);
+        q = nullptr;
+      }
+    p = nullptr;
+  }
+
+  int device_;
+  std::vector<void*> bufs_;
+  long long cap_ = 0, left_cap_ = 0;
+  int ndim_ = 0, left_ndim_ = 0;
+  int nint_cap_ = 0;
+  size_t slab_bytes_ = 0, heap_ints_ = 0;
+  size_t bytes_ = 0;
+  std::string err_;
+  Stats stats_;
+};
+
+inline int sm_count(int device) {
+  int n = 0;
+  cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, device);
+  return n > 0 ? n : 148;
+}
+
+// Divisions per axis of the initial grid (GPUKernelquad.cu:300-311).
+inline int grid_divisions(int ndim) { return ndim > 10 ? 1 : (ndim >= 5 ? 2 : 4); }
+
+template <int N, int K, class Src>
+inline void launch_eval(const Src& src, const RuleTables& T, const EngineArgs& a, int sms,
+                        cudaStream_t s) {
+  const long long threads = (long long)a.n * K;
+  long long blocks = (threads + 255) / 256;
+  blocks = std::max<long long>(1, std::min<long long>(blocks, (long long)sms * 32));
+  k_eval<N, K, Src><<<(unsigned)blocks, 256, 0, s>>>(src, T, a);
+}
+
+// Run one batch: `nint` integrals of one family and dimension N, all
+// starting from the unit cube.  Results go to out[0..nint).
+template <int N, class Src>
+int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
+              const double* epsabs, const Options& opt, Result* out, cudaStream_t s) {
+  static_assert(N >= 2 && N <= kMaxDim, "dimension out of range");
+  if (nint <= 0) return kErrInvalid;
+  const RuleTables T = make_rule9_tables(N);
+  const int sms = sm_count(ws.device());
+  const int dv = grid_divisions(N);
+  int per = 1;
+  for (int d = 0; d < N; ++d) per *= dv;
+  const int padded = (per + 31) & ~31;
+  long long n_cur = (long long)nint * padded;
+
+  if (!ws.reserve_integrals(nint)) return kErrCuda;
+  if (!ws.reserve_lists(N, std::max<long long>(n_cur, 2 * n_cur), 0, 0, s)) return kErrCuda;
+  if (!ws.reserve_leftovers(N, 1, 0, s)) return kErrCuda;
+
+  // integral states
+  std::vector<IntegralState> h(nint);
+  for (int k = 0; k < nint; ++k) {
+    IntegralState& is = h[k];
+    std::memset(&is, 0, sizeof(is));
+    is.epsrel = epsrel[k];
+    is.epsabs = epsabs[k];
+    is.state = kStateRunning;
+    is.seg_start = k * padded;
+    is.seg_count = per;
+  }
+  if (!ws.ck(cudaMemcpyAsync(ws.ist, h.data(), sizeof(IntegralState) * nint,
+                             cudaMemcpyHostToDevice, s)))
+    return kErrCuda;
+  Control c0;
+  std::memset(&c0, 0, sizeof(c0));
+  c0.n_cur = (int)n_cur;
+  if (!ws.ck(cudaMemcpyAsync(ws.ctl, &c0, sizeof(Control), cudaMemcpyHostToDevice, s)))
+    return kErrCuda;
+  ws.stats().h2d_bytes += (long long)(sizeof(IntegralState) * nint + sizeof(Control));
+
+  int cur = 0;
+  EngineArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.ist = ws.ist;
+  a.nint = nint;
+  a.ctl = ws.ctl;
+  a.policy = opt.policy;
+  a.phase1_cap = opt.policy == kPolicyReference ? opt.phase1_cap : 0;
+  a.max_iters = opt.max_iters;
+  a.npoints = T.npoints;
+  auto bind = [&](long long n) {
+    a.lo = ws.lo[cur];
+    a.len = ws.len[cur];
+    a.rid = ws.rid[cur];
+    a.n = (int)n;
+    a.cap = ws.cap();
+    a.avg = ws.avg;
+    a.err = ws.err;
+    a.axis = ws.axis;
+    a.active = ws.active;
+    a.part = ws.part;
+    a.chunk_excl = ws.chunk_excl;
+    a.nlo = ws.lo[cur ^ 1];
+    a.nlen = ws.len[cur ^ 1];
+    a.nrid = ws.rid[cur ^ 1];
+    a.ncap = ws.cap();
+    a.left_lo = ws.left_lo;
+    a.left_len = ws.left_len;
+    a.left_rid = ws.left_rid;
+    a.left_cap = ws.left_cap();
+  };
+  bind(n_cur);
+  {
+    const long long blocks = std::min<long long>((n_cur + 255) / 256, (long long)sms * 8);
+    k_init_grid<N><<<(unsigned)std::max<long long>(blocks, 1), 256, 0, s>>>(a, dv, per, padded);
+  }
+  ws.stats().launches += 1;
+  Stats& st = ws.stats();
+  long long n_left = 0;
+  int status = kOk;
+  for (int it = 0;; ++it) {
+    // capacity for the worst case of this iteration
+    const long long need = 2 * n_cur + 32ll * nint;
+    if (need > opt.max_slots) {
+      status = kErrCapacity;
+      break;
+    }
+    if (!ws.reserve_lists(N, need, cur, n_cur, s)) return kErrCuda;
+    if (opt.policy == kPolicyReference &&
+        !ws.reserve_leftovers(N, n_left + 2 * n_cur + 1, n_left, s))
+      return kErrCuda;
+    bind(n_cur);
+    int K = opt.lanes;
+    if (K <= 0) K = n_cur >= (long long)sms * 512 ? 1 : (n_cur >= (long long)sms * 64 ? 8 : 32);
+    if (ws.timing) ws.ck(cudaEventRecord(ws.ev[0], s));
+    switch (K) {
+      case 1: launch_eval<N, 1>(src, T, a, sms, s); break;
+      case 8: launch_eval<N, 8>(src, T, a, sms, s); break;
+      default: launch_eval<N, 32>(src, T, a, sms, s); break;
+    }
+    if (ws.timing) ws.ck(cudaEventRecord(ws.ev[1], s));
+    st.eval_launches += 1;
+    st.launches += 1;
+    st.regions_evaluated += n_cur;
+    const long long nchunk = (n_cur + 31) / 32;
+    const unsigned pb = (unsigned)std::max<long long>(1, std::min<long long>((nchunk + 7) / 8, sms * 16ll));
+    k_partials<<<pb, 256, 0, s>>>(a);
+    const unsigned db = (unsigned)std::max(1, std::min((nint + 7) / 8, sms * 16));
+    k_decide<<<db, 256, 0, s>>>(a);
+    k_scan<<<1, 1024, 0, s>>>(a);
+    k_split<N><<<pb, 256, 0, s>>>(a);
+    k_advance<<<(unsigned)std::max(1, std::min((nint + 255) / 256, sms)), 256, 0, s>>>(a);
+    st.launches += 5;
+    if (!ws.ck(cudaMemcpyAsync(ws.ctl_host_, ws.ctl, sizeof(Control), cudaMemcpyDeviceToHost, s)))
+      return kErrCuda;
+    if (!ws.ck(cudaStreamSynchronize(s))) return kErrCuda;
+    const Control c = *ws.ctl_host_;
+    st.iterations += 1;
+    st.d2h_bytes += (long long)sizeof(Control);
+    if (ws.timing) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, ws.ev[0], ws.ev[1]);
+      st.ms_eval += ms;
+    }
+    if (c.overflow) {
+      status = kErrCapacity;
+      break;
+    }
+    n_left = c.n_left;
+    n_cur = c.n_cur;
+    cur ^= 1;
+    if (c.n_running == 0 || n_cur == 0) break;
+  }
+
+  if (status == kOk && n_left > 0) {
+    // phase 2 on the leftover boxes
+    int dev_blocks = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&dev_blocks, k_phase2<N, Src>, 128, 0);
+    dev_blocks = std::max(1, dev_blocks);
+    long long blocks = std::min<long long>((long long)sms * dev_blocks, (n_left + 3) / 4);
+    blocks = std::max<long long>(blocks, 1);
+    const long long nwarps = blocks * 4;
+    const int stride = opt.phase2_max_regions + 2;
+    if (!ws.reserve_slab(sizeof(P2Region<N>) * nwarps * stride, (size_t)nwarps * stride))
+      return kErrCuda;
+    if (!ws.ck(cudaMemsetAsync(ws.counter, 0, sizeof(int), s))) return kErrCuda;
+    Phase2Args p;
+    p.left_lo = ws.left_lo;
+    p.left_len = ws.left_len;
+    p.left_rid = ws.left_rid;
+    p.left_cap = ws.left_cap();
+    p.n_left = (int)n_left;
+    p.max_regions = opt.phase2_max_regions;
+    p.slab = ws.slab;
+    p.heap = ws.heap;
+    p.next_box = ws.counter;
+    p.out = ws.left_res;
+    p.ist = ws.ist;
+    if (ws.timing) ws.ck(cudaEventRecord(ws.ev[2], s));
+    k_phase2<N, Src><<<(unsigned)blocks, 128, 0, s>>>(src, T, p);
+    if (ws.timing) ws.ck(cudaEventRecord(ws.ev[3], s));
+    st.phase2_boxes += n_left;
+    const unsigned cb = (unsigned)std::max(1, std::min((nint + 7) / 8, sms * 16));
+    k_phase2_collect<<<cb, 256, 0, s>>>(ws.ist, nint, ws.left_res, T.npoints);
+    st.launches += 2;
+  }
+
+  if (!ws.ck(cudaMemcpyAsync(h.data(), ws.ist, sizeof(IntegralState) * nint,
+                             cudaMemcpyDeviceToHost, s)))
+    return kErrCuda;
+  ws.stats().d2h_bytes += (long long)(sizeof(IntegralState) * nint);
+  if (!ws.ck(cudaStreamSynchronize(s))) return kErrCuda;
+  if (!ws.ck(cudaGetLastError())) return kErrCuda;
+  if (ws.timing && status == kOk && n_left > 0) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ws.ev[2], ws.ev[3]);
+    st.ms_phase2 += ms;
+  }
+  for (int k = 0; k < nint; ++k) {
+    const IntegralState& is = h[k];
+    Result& r = out[k];
+    r.nregions = is.nregions;
+    r.neval = is.neval;
+    r.iterations = is.iters;
+    r.state = is.state;
+    r.pad = 0;
+    if (is.state == kStateRunning || is.state == kStateCapacity) {
+      // stopped early: report the last full estimate, not converged
+      r.value = is.last_value;
+      r.error = is.last_error;
+      r.status = is.last_error <= detail::max_err(is.last_value, is.epsrel, is.epsabs) ? 0 : 1;
+    } else {
+      r.value = is.value;
+      r.error = is.error;
+      r.status = is.status;
+    }
+  }
+  return status;
+}
+
+}  // namespace cubature

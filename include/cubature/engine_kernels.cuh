@@ -1,0 +1,487 @@
+// engine_kernels.cuh -- the device side of the breadth-first engine.
+//
+// One iteration of the reference's first phase (GPUKernelquad.cu:509-605)
+// over a batch of independent integrals whose regions share one list:
+//
+//   eval      rule + fourth difference + error + classification per region
+//             (INTEGRATE_GPU_PHASE1, GPUQuadPhases.cu:38-79)
+//   partials  per 32-region chunk: value/error sums, finished sums, active
+//             count (the reference's four thrust::reduce calls and the
+//             exclusive scan, GPUKernelquad.cu:364-386,565-577)
+//   decide    per integral: totals, the global stop test, the child count
+//             (GPUKernelquad.cu:583-598)
+//   scan      exclusive scan of child counts over integrals -> new segments
+//   split     compaction + bisection of the active regions, written as
+//             adjacent children (alignRegions + divideIntervalsGPU,
+//             GPUKernelquad.cu:63-149)
+//
+// Layout in HBM: region lists are SoA, lo[d * cap + i] and len[d * cap + i]
+// (FP64), rid[i] = owning integral (-1 = padding).  Each integral owns a
+// contiguous segment whose start is a multiple of 32, so a 32-region chunk
+// never straddles two integrals and every reduction is a fixed-order tree
+// (results are bit-reproducible run to run).
+#pragma once
+
+#include <cstdint>
+
+#include "integrands.cuh"
+#include "region_rule.cuh"
+
+namespace cubature {
+
+enum Policy : int { kPolicyReference = 0, kPolicyBreadth = 1 };
+
+enum IntegralStateCode : int {
+  kStateRunning = 0,
+  kStateDone = 1,      // converged or out of active regions
+  kStatePhase2 = 2,    // handed to the depth-first second phase
+  kStateCapacity = 3,  // stopped: region capacity or iteration limit
+};
+
+// Per-integral state, resident on the device for the whole run.
+struct IntegralState {
+  double epsrel, epsabs;
+  double value, error;  // finished sums (final results when done)
+  double last_value, last_error;
+  unsigned long long nregions, neval;
+  int state, status, iters;
+  int left_new;                // leftover boxes produced this iteration
+  int seg_start, seg_count;    // segment in the current list
+  int next_start, next_count;  // segment in the next list
+  int left_start, left_count;  // leftover boxes for phase 2
+};
+
+struct ChunkPartial {
+  double sum_avg, sum_err;  // all regions of the chunk
+  double fin_avg, fin_err;  // finished regions only
+  int nactive, pad;
+};
+
+// Control block: list sizes and counters of the current iteration.
+struct Control {
+  int n_cur;      // slots in the current list (padded)
+  int n_next;     // slots in the next list (padded)
+  int n_running;  // integrals still running after this iteration
+  int n_left;     // leftover boxes queued for phase 2 so far
+  int overflow;   // set when a list would exceed its capacity
+  int iter;
+  int pad[2];
+};
+
+struct EngineArgs {
+  // current list
+  const double* lo;
+  const double* len;
+  const int* rid;
+  int n;  // padded slot count
+  long long cap;
+  // per-region outputs
+  double* avg;
+  double* err;
+  int* axis;
+  int* active;
+  // chunk partials / prefix
+  ChunkPartial* part;
+  int* chunk_excl;
+  // next list
+  double* nlo;
+  double* nlen;
+  int* nrid;
+  long long ncap;
+  // leftovers for phase 2
+  double* left_lo;
+  double* left_len;
+  int* left_rid;
+  long long left_cap;
+  // integrals
+  IntegralState* ist;
+  int nint;
+  Control* ctl;
+  int policy;
+  int phase1_cap;  // child count that ends phase 1 (0 = never)
+  int max_iters;   // phase-1 iteration limit
+  int npoints;
+};
+
+namespace detail {
+
+__host__ __device__ __forceinline__ double max_err(double avg, double epsrel, double epsabs) {
+  const double a = epsrel * fabs(avg);
+  return a > epsabs ? a : epsabs;
+}
+
+template <class F>
+struct SingleSource {
+  F f;
+  __device__ __forceinline__ const F& get(int) const { return f; }
+};
+
+template <class F>
+struct ParamSource {
+  const GenzParams* params;
+  __device__ __forceinline__ F get(int k) const { return F::load(params[k]); }
+};
+
+}  // namespace detail
+
+// ---------------------------------------------------------------------------
+// eval: K lanes per region, grid-stride over slots.
+// ---------------------------------------------------------------------------
+template <int N, int K, class Src>
+__global__ void __launch_bounds__(256) k_eval(Src src, RuleTables T, EngineArgs a) {
+  __shared__ detail::ItemTable<N> tab;
+  if (threadIdx.x == 0) tab.fill();
+  __syncthreads();
+
+  constexpr int kGroups = 256 / K;
+  const int lane = threadIdx.x % K;
+  const unsigned gmask = (K == 32) ? 0xffffffffu : (((1u << K) - 1u) << ((threadIdx.x & 31) & ~(K - 1)));
+  for (long long slot = (long long)blockIdx.x * kGroups + threadIdx.x / K; slot < a.n;
+       slot += (long long)gridDim.x * kGroups) {
+    const int k = a.rid[slot];
+    if (k < 0) {
+      if (lane == 0) {
+        a.avg[slot] = 0;
+        a.err[slot] = 0;
+        a.axis[slot] = 0;
+        a.active[slot] = 0;
+      }
+      continue;
+    }
+    double L[N], H[N];
+#pragma unroll
+    for (int d = 0; d < N; ++d) {
+      L[d] = a.lo[(long long)d * a.cap + slot];
+      H[d] = a.len[(long long)d * a.cap + slot];
+    }
+    const auto f = src.get(k);
+    detail::RegionSums rs;
+    detail::region_point_sums<N, K>(f, L, H, lane, tab, T.ratio, rs);
+    if (K > 1) detail::reduce_lanes<K>(rs, gmask);
+    if (lane == 0) {
+      double jac = 1;
+#pragma unroll
+      for (int d = 0; d < N; ++d) jac = __dmul_rn(jac, H[d]);
+      const detail::RegionResult r = detail::finish_region<N>(rs, T, jac, 0);
+      const IntegralState& is = a.ist[k];
+      // reference policy: fail when err / max(epsrel|avg|, epsabs) > 1
+      const double ratio = r.err / detail::max_err(r.avg, is.epsrel, is.epsabs);
+      a.avg[slot] = r.avg;
+      a.err[slot] = r.err;
+      a.axis[slot] = r.axis;
+      a.active[slot] = ratio > 1;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// partials: one warp per 32-slot chunk.
+// ---------------------------------------------------------------------------
+static __global__ void __launch_bounds__(256) k_partials(EngineArgs a) {
+  const int lane = threadIdx.x & 31;
+  const long long nchunk = (a.n + 31) / 32;
+  for (long long c = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / 32; c < nchunk;
+       c += (long long)gridDim.x * blockDim.x / 32) {
+    const long long i = c * 32 + lane;
+    const bool valid = i < a.n && a.rid[i] >= 0;
+    const double av = valid ? a.avg[i] : 0.0, er = valid ? a.err[i] : 0.0;
+    const bool act = valid && a.active[i];
+    double s0 = av, s1 = er, s2 = act ? 0.0 : av, s3 = act ? 0.0 : er;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      s0 += __shfl_xor_sync(0xffffffffu, s0, off);
+      s1 += __shfl_xor_sync(0xffffffffu, s1, off);
+      s2 += __shfl_xor_sync(0xffffffffu, s2, off);
+      s3 += __shfl_xor_sync(0xffffffffu, s3, off);
+    }
+    const unsigned b = __ballot_sync(0xffffffffu, act);
+    if (lane == 0) {
+      ChunkPartial p;
+      p.sum_avg = s0;
+      p.sum_err = s1;
+      p.fin_avg = s2;
+      p.fin_err = s3;
+      p.nactive = __popc(b);
+      p.pad = 0;
+      a.part[c] = p;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// decide: one warp per running integral.
+// ---------------------------------------------------------------------------
+static __global__ void __launch_bounds__(256) k_decide(EngineArgs a) {
+  const int lane = threadIdx.x & 31;
+  for (int k = (blockIdx.x * blockDim.x + threadIdx.x) / 32; k < a.nint;
+       k += gridDim.x * blockDim.x / 32) {
+    IntegralState& is = a.ist[k];
+    if (is.state != kStateRunning) {
+      if (lane == 0) {
+        is.next_count = 0;
+        is.left_new = 0;
+      }
+      continue;
+    }
+    const int c0 = is.seg_start / 32;
+    const int nc = (is.seg_count + 31) / 32;
+    double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+    for (int c = lane; c < nc; c += 32) {
+      const ChunkPartial p = a.part[c0 + c];
+      s0 += p.sum_avg;
+      s1 += p.sum_err;
+      s2 += p.fin_avg;
+      s3 += p.fin_err;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      s0 += __shfl_xor_sync(0xffffffffu, s0, off);
+      s1 += __shfl_xor_sync(0xffffffffu, s1, off);
+      s2 += __shfl_xor_sync(0xffffffffu, s2, off);
+      s3 += __shfl_xor_sync(0xffffffffu, s3, off);
+    }
+    // exclusive scan of active counts over the integral's chunks
+    int running = 0;
+    for (int base = 0; base < nc; base += 32) {
+      const int c = base + lane;
+      const int v = c < nc ? a.part[c0 + c].nactive : 0;
+      int incl = v;
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane >= off) incl += t;
+      }
+      if (c < nc) a.chunk_excl[c0 + c] = running + incl - v;
+      running += __shfl_sync(0xffffffffu, incl, 31);
+    }
+    if (lane == 0) {
+      const int m = running;
+      const double rG = is.value + s0, errG = is.error + s1;
+      is.value += s2;
+      is.error += s3;
+      is.last_value = rG;
+      is.last_error = errG;
+      is.nregions += (unsigned long long)is.seg_count;
+      is.neval += (unsigned long long)is.seg_count * (unsigned long long)a.npoints;
+      is.iters += 1;
+      is.next_count = 0;
+      is.left_new = 0;
+      if (errG <= detail::max_err(rG, is.epsrel, is.epsabs)) {
+        // global stop test (GPUKernelquad.cu:583-598)
+        is.value = rG;
+        is.error = errG;
+        is.state = kStateDone;
+        is.status = 0;
+      } else if (m == 0) {
+        // every region finished on its own tolerance
+        is.state = kStateDone;
+        is.status = 0;
+      } else {
+        const long long children = 2ll * m;
+        const bool cap_hit = a.phase1_cap > 0 && children >= a.phase1_cap;
+        const bool iter_hit = is.iters >= a.max_iters;
+        if (cap_hit || iter_hit) {
+          if (a.policy == kPolicyReference) {
+            is.state = kStatePhase2;
+            is.left_new = (int)children;
+          } else {
+            is.state = kStateCapacity;
+            is.value = rG;
+            is.error = errG;
+            is.status = 1;
+          }
+        } else {
+          is.next_count = (int)children;
+        }
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// scan: one block assigns the next segments and leftover ranges.
+// ---------------------------------------------------------------------------
+static __global__ void __launch_bounds__(1024) k_scan(EngineArgs a) {
+  __shared__ int warp_tot[32][2];
+  __shared__ int carry[2];
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  if (tid == 0) {
+    carry[0] = 0;
+    carry[1] = a.ctl->n_left;
+  }
+  __syncthreads();
+  int nrun = 0;
+  for (int base = 0; base < a.nint; base += 1024) {
+    const int k = base + tid;
+    int vn = 0, vl = 0;
+    if (k < a.nint) {
+      const IntegralState& is = a.ist[k];
+      vn = (is.next_count + 31) & ~31;  // padded segment
+      vl = is.left_new;
+      nrun += is.state == kStateRunning && is.next_count > 0;
+    }
+    int in = vn, il = vl;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const int tn = __shfl_up_sync(0xffffffffu, in, off);
+      const int tl = __shfl_up_sync(0xffffffffu, il, off);
+      if (lane >= off) { in += tn; il += tl; }
+    }
+    if (lane == 31) { warp_tot[wid][0] = in; warp_tot[wid][1] = il; }
+    __syncthreads();
+    if (wid == 0) {
+      int wn = warp_tot[lane][0], wl = warp_tot[lane][1];
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const int tn = __shfl_up_sync(0xffffffffu, wn, off);
+        const int tl = __shfl_up_sync(0xffffffffu, wl, off);
+        if (lane >= off) { wn += tn; wl += tl; }
+      }
+      warp_tot[lane][0] = wn;
+      warp_tot[lane][1] = wl;
+    }
+    __syncthreads();
+    const int wbase_n = wid > 0 ? warp_tot[wid - 1][0] : 0;
+    const int wbase_l = wid > 0 ? warp_tot[wid - 1][1] : 0;
+    if (k < a.nint) {
+      IntegralState& is = a.ist[k];
+      is.next_start = carry[0] + wbase_n + in - vn;
+      if (vl > 0) {
+        is.left_start = carry[1] + wbase_l + il - vl;
+        is.left_count = vl;
+      }
+    }
+    __syncthreads();
+    if (tid == 0) {
+      carry[0] += warp_tot[31][0];
+      carry[1] += warp_tot[31][1];
+    }
+    __syncthreads();
+  }
+  // count running integrals
+  __shared__ int nrun_s;
+  if (tid == 0) nrun_s = 0;
+  __syncthreads();
+  atomicAdd(&nrun_s, nrun);
+  __syncthreads();
+  if (tid == 0) {
+    Control* c = a.ctl;
+    c->n_next = carry[0];
+    c->n_left = carry[1];
+    c->n_running = nrun_s;
+    c->overflow = (carry[0] > a.ncap) || (carry[1] > a.left_cap);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// split: one warp per chunk; writes two adjacent children per active
+// region, to the next list (running integrals) or the leftover list
+// (integrals handed to phase 2).  Also writes the padding slot ids.
+// ---------------------------------------------------------------------------
+template <int N>
+__global__ void __launch_bounds__(256) k_split(EngineArgs a) {
+  if (a.ctl->overflow) return;
+  const int lane = threadIdx.x & 31;
+  const long long nchunk = (a.n + 31) / 32;
+  const long long gwarp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / 32;
+  const long long nwarp = (long long)gridDim.x * blockDim.x / 32;
+  for (long long c = gwarp; c < nchunk; c += nwarp) {
+    const long long i = c * 32 + lane;
+    const int k = i < a.n ? a.rid[i] : -1;
+    bool act = k >= 0 && a.active[i];
+    int state = kStateDone;
+    if (act) {
+      state = a.ist[k].state;
+      act = (state == kStateRunning && a.ist[k].next_count > 0) ||
+            (state == kStatePhase2 && a.ist[k].left_new > 0);
+    }
+    const unsigned b = __ballot_sync(0xffffffffu, act);
+    if (!act) continue;
+    const int rank = a.chunk_excl[c] + __popc(b & ((1u << lane) - 1u));
+    const int ax = a.axis[i];
+    double* dlo;
+    double* dlen;
+    int* drid;
+    long long dcap, dst;
+    if (state == kStatePhase2) {
+      dlo = a.left_lo; dlen = a.left_len; drid = a.left_rid; dcap = a.left_cap;
+      dst = a.ist[k].left_start + 2ll * rank;
+    } else {
+      dlo = a.nlo; dlen = a.nlen; drid = a.nrid; dcap = a.ncap;
+      dst = a.ist[k].next_start + 2ll * rank;
+    }
+#pragma unroll
+    for (int d = 0; d < N; ++d) {
+      const double l = a.lo[(long long)d * a.cap + i];
+      const double w = a.len[(long long)d * a.cap + i];
+      if (d == ax) {
+        const double h = w / 2;
+        dlo[(long long)d * dcap + dst] = l;
+        dlo[(long long)d * dcap + dst + 1] = l + 1 * h;
+        dlen[(long long)d * dcap + dst] = h;
+        dlen[(long long)d * dcap + dst + 1] = h;
+      } else {
+        dlo[(long long)d * dcap + dst] = l;
+        dlo[(long long)d * dcap + dst + 1] = l;
+        dlen[(long long)d * dcap + dst] = w;
+        dlen[(long long)d * dcap + dst + 1] = w;
+      }
+    }
+    drid[dst] = k;
+    drid[dst + 1] = k;
+  }
+  // padding ids of the next list (<= 31 per integral)
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < a.nint;
+       k += (long long)gridDim.x * blockDim.x) {
+    const IntegralState& is = a.ist[k];
+    if (is.next_count <= 0) continue;
+    const int padded = (is.next_count + 31) & ~31;
+    for (int j = is.next_count; j < padded; ++j) a.nrid[is.next_start + j] = -1;
+  }
+}
+
+// After split: the next list becomes current.
+static __global__ void k_advance(EngineArgs a) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < a.nint; k += gridDim.x * blockDim.x) {
+    IntegralState& is = a.ist[k];
+    if (is.state == kStateRunning) {
+      is.seg_start = is.next_start;
+      is.seg_count = is.next_count;
+      if (is.next_count == 0) is.state = kStateDone;
+    } else {
+      is.seg_count = 0;
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.ctl->n_cur = a.ctl->n_next;
+    a.ctl->iter += 1;
+  }
+}
+
+// Initial grid for every integral: d^N equal boxes of the unit cube
+// (GPUKernelquad.cu:24-61,300-316), dimension 0 varying fastest.
+template <int N>
+__global__ void k_init_grid(EngineArgs a, int divisions, int per_integral, int padded) {
+  const long long total = (long long)a.nint * padded;
+  const double w = 1.0 / divisions;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(t / padded);
+    const int j = (int)(t % padded);
+    if (j >= per_integral) {
+      const_cast<int*>(a.rid)[t] = -1;
+      continue;
+    }
+    int rem = j;
+#pragma unroll
+    for (int d = 0; d < N; ++d) {
+      const int id = rem % divisions;
+      rem /= divisions;
+      const_cast<double*>(a.lo)[(long long)d * a.cap + t] = 0 + id * w;
+      const_cast<double*>(a.len)[(long long)d * a.cap + t] = w;
+    }
+    const_cast<int*>(a.rid)[t] = k;
+  }
+}
+
+}  // namespace cubature

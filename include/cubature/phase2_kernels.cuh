@@ -1,0 +1,282 @@
+// phase2_kernels.cuh -- depth-first refinement of leftover boxes.
+//
+// The reference's second phase (BLOCK_INTEGRATE_GPU_PHASE2,
+// quad/GPUquad/GPUQuadPhases.cu:424-536) refines every box left over by the
+// first phase on its own: serial Cuhre with the box's own tolerance
+// (ERR <= max(epsrel |RESULT|, epsabs)) and at most 2048 bisections.
+//
+// Re-design for sm_100a: one warp per leftover box, persistent warps pulling
+// boxes from an atomic counter.  Each step bisects the box's exact maximum
+// error subregion (a binary heap kept by lane 0), and the two children are
+// evaluated in parallel by the two 16-lane halves of the warp.  Subregions
+// live in a per-warp slab of global memory preallocated by the host, so
+// there is no device malloc and the footprint is fixed by the grid size.
+// Every loop is bounded (at most max_regions steps per box).
+#pragma once
+
+#include "engine_kernels.cuh"
+
+namespace cubature {
+
+struct LeftoverResult {
+  double value, error;
+  int nregions, failed;
+};
+
+// One subregion of a leftover box, in the box's local [0,1]^N coordinates.
+template <int N>
+struct P2Region {
+  double avg, err;
+  int axis, div;
+  double lo[N], hi[N];
+};
+
+struct Phase2Args {
+  const double* left_lo;  // [N][left_cap]
+  const double* left_len;
+  const int* left_rid;
+  long long left_cap;
+  int n_left;
+  int max_regions;  // bisections per box (MAX_GLOBALPOOL_SIZE, quad.h:9)
+  void* slab;       // per-warp pools: nwarps * (max_regions + 2) regions
+  int* heap;        // per-warp heaps: nwarps * (max_regions + 2) ints
+  int* next_box;    // work counter
+  LeftoverResult* out;
+  const IntegralState* ist;
+};
+
+namespace detail {
+
+template <int N>
+__device__ __forceinline__ void heap_push(P2Region<N>* pool, int* heap, int& hn, int idx) {
+  int i = hn++;
+  heap[i] = idx;
+  while (i > 0) {
+    const int p = (i - 1) / 2;
+    if (pool[heap[p]].err >= pool[heap[i]].err) break;
+    const int t = heap[p];
+    heap[p] = heap[i];
+    heap[i] = t;
+    i = p;
+  }
+}
+
+template <int N>
+__device__ __forceinline__ int heap_pop(P2Region<N>* pool, int* heap, int& hn) {
+  const int top = heap[0];
+  heap[0] = heap[--hn];
+  int i = 0;
+  for (;;) {
+    const int l = 2 * i + 1, r = l + 1;
+    int m = i;
+    if (l < hn && pool[heap[l]].err > pool[heap[m]].err) m = l;
+    if (r < hn && pool[heap[r]].err > pool[heap[m]].err) m = r;
+    if (m == i) break;
+    const int t = heap[m];
+    heap[m] = heap[i];
+    heap[i] = t;
+    i = m;
+  }
+  return top;
+}
+
+// Evaluate subregion `reg` of box (BL, BW) with the 16 lanes of a half warp.
+template <int N, class F>
+__device__ __forceinline__ RegionResult eval_sub(const F& f, const double (&BL)[N],
+                                                 const double (&BW)[N], const P2Region<N>& reg,
+                                                 int hlane, unsigned hmask, const ItemTable<N>& tab,
+                                                 const RuleTables& T) {
+  double L[N], H[N];
+  int widest = 0;
+  double wmax = 0;
+#pragma unroll
+  for (int d = 0; d < N; ++d) {
+    L[d] = fma(reg.lo[d], BW[d], BL[d]);
+    H[d] = (reg.hi[d] - reg.lo[d]) * BW[d];
+    const double w = reg.hi[d] - reg.lo[d];
+    if (w > wmax) {  // widest local side (GPUQuadSample.cu:118-125)
+      wmax = w;
+      widest = d;
+    }
+  }
+  RegionSums rs;
+  region_point_sums<N, 16>(f, L, H, hlane, tab, T.ratio, rs);
+  reduce_lanes<16>(rs, hmask);
+  double jac = 1;
+#pragma unroll
+  for (int d = 0; d < N; ++d) jac = __dmul_rn(jac, H[d]);
+  return finish_region<N>(rs, T, jac, widest);
+}
+
+}  // namespace detail
+
+template <int N, class Src>
+__global__ void __launch_bounds__(128) k_phase2(Src src, RuleTables T, Phase2Args a) {
+  __shared__ detail::ItemTable<N> tab;
+  if (threadIdx.x == 0) tab.fill();
+  __syncthreads();
+
+  const int lane = threadIdx.x & 31;
+  const int half = lane >> 4, hlane = lane & 15;
+  const unsigned hmask = half ? 0xffff0000u : 0x0000ffffu;
+  const long long gwarp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / 32;
+  const int stride = a.max_regions + 2;
+  P2Region<N>* pool = reinterpret_cast<P2Region<N>*>(a.slab) + gwarp * stride;
+  int* heap = a.heap + gwarp * stride;
+
+  for (;;) {
+    int box = 0;
+    if (lane == 0) box = atomicAdd(a.next_box, 1);
+    box = __shfl_sync(0xffffffffu, box, 0);
+    if (box >= a.n_left) break;
+    const int k = a.left_rid[box];
+    const IntegralState& is = a.ist[k];
+    const double epsrel = is.epsrel, epsabs = is.epsabs;
+    double BL[N], BW[N];
+#pragma unroll
+    for (int d = 0; d < N; ++d) {
+      BL[d] = a.left_lo[(long long)d * a.left_cap + box];
+      BW[d] = a.left_len[(long long)d * a.left_cap + box];
+    }
+    const auto f = src.get(k);
+
+    // the whole box as the first subregion (INIT_REGION_POOL, :110-182)
+    P2Region<N> r0;
+#pragma unroll
+    for (int d = 0; d < N; ++d) { r0.lo[d] = 0; r0.hi[d] = 1; }
+    r0.div = 0;
+    {
+      // both halves evaluate it; half 0's result is used
+      const detail::RegionResult rr = detail::eval_sub<N>(f, BL, BW, r0, hlane, hmask, tab, T);
+      r0.avg = rr.avg;
+      r0.err = rr.err;
+      r0.axis = rr.axis;
+    }
+    int hn = 0, used = 1;
+    double ERR = r0.err, RESULT = r0.avg;
+    if (lane == 0) {
+      pool[0] = r0;
+      detail::heap_push<N>(pool, heap, hn, 0);
+    }
+    __syncwarp();
+    int nreg = 1;
+    for (; nreg <= a.max_regions &&
+           (nreg == 1 || ERR > detail::max_err(RESULT, epsrel, epsabs));
+         ++nreg) {
+      int pi = 0;
+      if (lane == 0) pi = detail::heap_pop<N>(pool, heap, hn);
+      pi = __shfl_sync(0xffffffffu, pi, 0);
+      __syncwarp();
+      const P2Region<N> parent = pool[pi];
+      P2Region<N> child = parent;
+      const int ax = parent.axis;
+      const double mid = 0.5 * (parent.lo[ax] + parent.hi[ax]);
+      child.div = parent.div + 1;
+#pragma unroll
+      for (int d = 0; d < N; ++d) {
+        if (d == ax) {
+          if (half == 0) child.hi[d] = mid;
+          else child.lo[d] = mid;
+        }
+      }
+      const detail::RegionResult rr = detail::eval_sub<N>(f, BL, BW, child, hlane, hmask, tab, T);
+      const double avgR = __shfl_sync(0xffffffffu, rr.avg, 16);
+      const double errR0 = __shfl_sync(0xffffffffu, rr.err, 16);
+      const int axR = __shfl_sync(0xffffffffu, rr.axis, 16);
+      if (lane == 0) {
+        // Cuhre error refinement (GPUQuadPhases.cu:498-515)
+        double errL = rr.err, errR = errR0;
+        const double diff = fabs(.25 * (rr.avg + avgR - parent.avg));
+        const double e = errL + errR;
+        if (e > 0) {
+          const double c = 1 + 2 * diff / e;
+          errL *= c;
+          errR *= c;
+        }
+        errL += diff;
+        errR += diff;
+        ERR += errL + errR - parent.err;
+        RESULT += rr.avg + avgR - parent.avg;
+        P2Region<N> left = parent, right = parent;
+        left.div = right.div = parent.div + 1;
+#pragma unroll
+        for (int d = 0; d < N; ++d) {
+          if (d == ax) {
+            left.hi[d] = mid;
+            right.lo[d] = mid;
+          }
+        }
+        left.avg = rr.avg;
+        left.err = errL;
+        left.axis = rr.axis;
+        right.avg = avgR;
+        right.err = errR;
+        right.axis = axR;
+        pool[pi] = left;
+        pool[used] = right;
+        detail::heap_push<N>(pool, heap, hn, pi);
+        detail::heap_push<N>(pool, heap, hn, used);
+      }
+      ++used;
+      ERR = __shfl_sync(0xffffffffu, ERR, 0);
+      RESULT = __shfl_sync(0xffffffffu, RESULT, 0);
+      __syncwarp();
+    }
+    if (lane == 0) {
+      int failed = ERR > detail::max_err(RESULT, epsrel, epsabs);
+      if (ERR > 1e10) {  // GPUQuadPhases.cu:519-527
+        RESULT = 0.0;
+        ERR = 0.0;
+        failed = 1;
+      }
+      LeftoverResult o;
+      o.value = RESULT;
+      o.error = ERR;
+      o.nregions = nreg;
+      o.failed = failed;
+      a.out[box] = o;
+    }
+    __syncwarp();
+  }
+}
+
+// Per-integral sums of the phase-2 results, one warp per integral, and the
+// final status (GPUKernelquad.cu:870-892, GPUquad.h:713-714).
+static __global__ void k_phase2_collect(IntegralState* ist, int nint, const LeftoverResult* res,
+                                 int npoints) {
+  const int lane = threadIdx.x & 31;
+  for (int k = (blockIdx.x * blockDim.x + threadIdx.x) / 32; k < nint;
+       k += gridDim.x * blockDim.x / 32) {
+    IntegralState& is = ist[k];
+    if (is.state != kStatePhase2) continue;
+    double v = 0, e = 0;
+    unsigned long long nr = 0;
+    int nf = 0;
+    for (int j = lane; j < is.left_count; j += 32) {
+      const LeftoverResult r = res[is.left_start + j];
+      v += r.value;
+      e += r.error;
+      nr += (unsigned long long)r.nregions;
+      nf += r.failed;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      v += __shfl_xor_sync(0xffffffffu, v, off);
+      e += __shfl_xor_sync(0xffffffffu, e, off);
+      nr += __shfl_xor_sync(0xffffffffu, nr, off);
+      nf += __shfl_xor_sync(0xffffffffu, nf, off);
+    }
+    if (lane == 0) {
+      const unsigned long long n = (unsigned long long)is.left_count;
+      is.value += v;
+      is.error += e;
+      is.nregions += nr;
+      is.neval += (nr - n) * (unsigned long long)npoints * 2ull + n * (unsigned long long)npoints;
+      is.status = nf;
+      if (is.error <= detail::max_err(is.value, is.epsrel, is.epsabs)) is.status = 0;
+      is.state = kStateDone;
+    }
+  }
+}
+
+}  // namespace cubature

@@ -1,0 +1,330 @@
+// capi.cu -- the C ABI (include/cubature.h): contexts, dispatch by
+// dimension and family, per-step entry points.
+#include <cstring>
+#include <string>
+
+#include "capi_internal.h"
+#include "cubature/step_kernels.cuh"
+
+namespace cubature {
+namespace capi {
+
+namespace {
+thread_local std::string g_error;
+}
+
+void set_error(const std::string& msg) { g_error = msg; }
+
+cudaStream_t as_stream(void* s) { return static_cast<cudaStream_t>(s); }
+
+Options to_options(const cub_options* opt) {
+  Options o;
+  if (!opt) return o;
+  o.policy = opt->policy;
+  if (opt->phase1_cap > 0) o.phase1_cap = opt->phase1_cap;
+  if (opt->max_iters > 0) o.max_iters = opt->max_iters;
+  if (opt->phase2_max_regions > 0) o.phase2_max_regions = opt->phase2_max_regions;
+  if (opt->max_slots > 0) o.max_slots = opt->max_slots;
+  o.lanes = opt->lanes;
+  return o;
+}
+
+namespace {
+
+bool check_ndim(int ndim) {
+  if (ndim < CUB_MIN_NDIM || ndim > CUB_MAX_NDIM) {
+    set_error("ndim " + std::to_string(ndim) + " outside the built range [" +
+              std::to_string(CUB_MIN_NDIM) + ", " + std::to_string(CUB_MAX_NDIM) + "]");
+    return false;
+  }
+  return true;
+}
+
+bool check_family(int family) {
+  if (family < CUB_GAUSSIAN || family > CUB_COSSUM) {
+    set_error("unknown integrand family " + std::to_string(family));
+    return false;
+  }
+  return true;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+  set_error(std::string(what) + ": " + cudaGetErrorString(e));
+  return CUB_ERR_CUDA;
+}
+
+int dispatch_run(cub_ctx* ctx, int family, int ndim, int count, const GenzParams* h,
+                 const GenzParams* d, const double* er, const double* ea, const Options& o,
+                 Result* out) {
+  switch (ndim) {
+    case 2: return run_dim_2(ctx, family, count, h, d, er, ea, o, out);
+    case 3: return run_dim_3(ctx, family, count, h, d, er, ea, o, out);
+    case 4: return run_dim_4(ctx, family, count, h, d, er, ea, o, out);
+    case 5: return run_dim_5(ctx, family, count, h, d, er, ea, o, out);
+    case 6: return run_dim_6(ctx, family, count, h, d, er, ea, o, out);
+    case 7: return run_dim_7(ctx, family, count, h, d, er, ea, o, out);
+    case 8: return run_dim_8(ctx, family, count, h, d, er, ea, o, out);
+  }
+  return CUB_ERR_INVALID;
+}
+
+void to_c(const Result& r, cub_result* c) {
+  c->value = r.value;
+  c->error = r.error;
+  c->nregions = r.nregions;
+  c->neval = r.neval;
+  c->status = r.status;
+  c->iterations = r.iterations;
+  c->state = r.state;
+  c->reserved = 0;
+}
+
+}  // namespace
+}  // namespace capi
+}  // namespace cubature
+
+using namespace cubature;
+using namespace cubature::capi;
+
+extern "C" {
+
+int cub_version(void) { return (0 << 16) | 1; }
+
+const char* cub_last_error(void) { return g_error.c_str(); }
+
+void cub_default_options(cub_options* opt) {
+  if (!opt) return;
+  const Options o;
+  std::memset(opt, 0, sizeof(*opt));
+  opt->policy = o.policy;
+  opt->phase1_cap = o.phase1_cap;
+  opt->max_iters = o.max_iters;
+  opt->phase2_max_regions = o.phase2_max_regions;
+  opt->max_slots = o.max_slots;
+  opt->lanes = o.lanes;
+}
+
+cub_ctx* cub_create(int device) {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) {
+    set_error(std::string("no CUDA device: ") + cudaGetErrorString(e));
+    return nullptr;
+  }
+  if (device < 0 || device >= n) {
+    set_error("device index out of range");
+    return nullptr;
+  }
+  if ((e = cudaSetDevice(device)) != cudaSuccess) {
+    set_error(std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+    return nullptr;
+  }
+  cub_ctx* ctx = new cub_ctx();
+  ctx->device = device;
+  if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess) {
+    set_error(std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
+    delete ctx;
+    return nullptr;
+  }
+  ctx->ws = new Workspace(device);
+  return ctx;
+}
+
+void cub_destroy(cub_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  delete ctx->ws;
+  if (ctx->d_params) cudaFree(ctx->d_params);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+size_t cub_ctx_bytes(const cub_ctx* ctx) { return ctx && ctx->ws ? ctx->ws->bytes_reserved() : 0; }
+
+void* cub_ctx_stream(cub_ctx* ctx) { return ctx ? static_cast<void*>(ctx->stream) : nullptr; }
+
+int cub_ctx_stats(const cub_ctx* ctx, cub_stats* out) {
+  if (!ctx || !out) {
+    set_error("invalid argument");
+    return CUB_ERR_INVALID;
+  }
+  const Stats& s = ctx->ws->stats();
+  out->ms_eval = s.ms_eval;
+  out->ms_phase2 = s.ms_phase2;
+  out->eval_launches = s.eval_launches;
+  out->launches = s.launches;
+  out->regions_evaluated = s.regions_evaluated;
+  out->iterations = s.iterations;
+  out->phase2_boxes = s.phase2_boxes;
+  out->h2d_bytes = s.h2d_bytes;
+  out->d2h_bytes = s.d2h_bytes;
+  return 0;
+}
+
+void cub_ctx_reset_stats(cub_ctx* ctx) {
+  if (ctx) ctx->ws->stats() = Stats();
+}
+
+void cub_ctx_set_timing(cub_ctx* ctx, int on) {
+  if (ctx) ctx->ws->timing = on != 0;
+}
+
+int cub_integrate_batch(cub_ctx* ctx, int family, int ndim, int count,
+                        const cub_genz_params* params, const double* epsrel,
+                        const double* epsabs, double epsrel0, double epsabs0,
+                        const cub_options* opt, cub_result* out) {
+  if (!ctx || !params || !out || count <= 0) {
+    set_error("invalid argument");
+    return CUB_ERR_INVALID;
+  }
+  if (!check_ndim(ndim) || !check_family(family)) return CUB_ERR_INVALID;
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+  static_assert(sizeof(cub_genz_params) == sizeof(GenzParams), "params layout");
+  const GenzParams* h = reinterpret_cast<const GenzParams*>(params);
+  std::vector<double> er(count), ea(count);
+  for (int k = 0; k < count; ++k) {
+    er[k] = epsrel ? epsrel[k] : epsrel0;
+    ea[k] = epsabs ? epsabs[k] : epsabs0;
+    if (!(er[k] >= 0) || !(ea[k] >= 0)) {
+      set_error("epsrel/epsabs must be >= 0");
+      return CUB_ERR_INVALID;
+    }
+  }
+  const GenzParams* d = nullptr;
+  if (count > 1) {
+    if (count > ctx->params_cap) {
+      if (ctx->d_params) cudaFree(ctx->d_params);
+      ctx->d_params = nullptr;
+      ctx->params_cap = 0;
+      if ((e = cudaMalloc(&ctx->d_params, sizeof(GenzParams) * count)) != cudaSuccess)
+        return cuda_fail(e, "cudaMalloc(params)");
+      ctx->params_cap = count;
+    }
+    if ((e = cudaMemcpyAsync(ctx->d_params, h, sizeof(GenzParams) * count,
+                             cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess)
+      return cuda_fail(e, "cudaMemcpyAsync(params)");
+    ctx->ws->stats().h2d_bytes += (long long)(sizeof(GenzParams) * count);
+    d = ctx->d_params;
+  }
+  const Options o = to_options(opt);
+  std::vector<Result> res(count);
+  const int rc = dispatch_run(ctx, family, ndim, count, h, d, er.data(), ea.data(), o, res.data());
+  if (rc == kErrCuda) {
+    set_error(ctx->ws->error());
+    return CUB_ERR_CUDA;
+  }
+  if (rc == kErrCapacity) set_error("region capacity exceeded; results are the last estimates");
+  if (rc < 0 && rc != kErrCapacity) return rc;
+  for (int k = 0; k < count; ++k) to_c(res[k], &out[k]);
+  return rc == kErrCapacity ? CUB_ERR_CAPACITY : 0;
+}
+
+int cub_integrate(cub_ctx* ctx, int family, int ndim, const cub_genz_params* params,
+                  double epsrel, double epsabs, const cub_options* opt, cub_result* out) {
+  return cub_integrate_batch(ctx, family, ndim, 1, params, nullptr, nullptr, epsrel, epsabs, opt,
+                             out);
+}
+
+int cub_rule_tables(int ndim, double* wt, double* scale, double* norm, int* count) {
+  if (ndim < 2 || ndim > CUB_MAXDIM) {
+    set_error("ndim out of range");
+    return CUB_ERR_INVALID;
+  }
+  const RuleTables T = make_rule9_tables(ndim);
+  if (wt) std::memcpy(wt, T.wt, sizeof(T.wt));
+  if (scale) std::memcpy(scale, T.scale, sizeof(T.scale));
+  if (norm) std::memcpy(norm, T.norm, sizeof(T.norm));
+  if (count) std::memcpy(count, T.count, sizeof(T.count));
+  return 0;
+}
+
+int cub_rule_eval(int family, int ndim, const cub_genz_params* params, long long n,
+                  const double* d_lo, const double* d_len, long long ld, double epsrel,
+                  double epsabs, double* d_avg, double* d_err, int* d_axis, int* d_active,
+                  void* stream) {
+  if (!check_ndim(ndim) || !check_family(family)) return CUB_ERR_INVALID;
+  if (!params || n < 0 || ld < n || (n > 0 && (!d_lo || !d_len || !d_avg || !d_err || !d_axis ||
+                                                 !d_active))) {
+    set_error("invalid argument");
+    return CUB_ERR_INVALID;
+  }
+  if (n == 0) return 0;
+  const GenzParams& p = *reinterpret_cast<const GenzParams*>(params);
+  const cudaStream_t s = as_stream(stream);
+  int rc = CUB_ERR_INVALID;
+  switch (ndim) {
+#define CUB_RULE_CASE(N)                                                                        \
+  case N:                                                                                      \
+    rc = rule_eval_dim_##N(family, p, n, d_lo, d_len, ld, epsrel, epsabs, d_avg, d_err, d_axis, \
+                           d_active, s);                                                       \
+    break;
+    CUB_RULE_CASE(2) CUB_RULE_CASE(3) CUB_RULE_CASE(4) CUB_RULE_CASE(5) CUB_RULE_CASE(6)
+    CUB_RULE_CASE(7) CUB_RULE_CASE(8)
+#undef CUB_RULE_CASE
+  }
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "rule kernel launch");
+  return rc;
+}
+
+size_t cub_split_scratch_bytes(long long n) {
+  const long long nchunk = (n + 31) / 32;
+  return sizeof(int) * 2 * (size_t)(nchunk + 1);
+}
+
+size_t cub_reduce_scratch_bytes(long long) { return sizeof(double) * 4 * kReduceBlocks; }
+
+int cub_split(int ndim, long long n, const double* d_lo, const double* d_len, long long ld,
+              const int* d_active, const int* d_axis, double* d_out_lo, double* d_out_len,
+              long long out_ld, int layout, long long* d_count, void* d_scratch,
+              size_t scratch_bytes, void* stream) {
+  if (!check_ndim(ndim)) return CUB_ERR_INVALID;
+  if (n < 0 || ld < n || !d_count || (layout != 0 && layout != 1) ||
+      scratch_bytes < cub_split_scratch_bytes(n) || (n > 0 && !d_scratch)) {
+    set_error("invalid argument");
+    return CUB_ERR_INVALID;
+  }
+  const cudaStream_t s = as_stream(stream);
+  if (n == 0) {
+    const cudaError_t e = cudaMemsetAsync(d_count, 0, sizeof(long long), s);
+    return e == cudaSuccess ? 0 : cuda_fail(e, "cudaMemsetAsync");
+  }
+  int* cnt = static_cast<int*>(d_scratch);
+  int* excl = cnt + (n + 31) / 32 + 1;
+  int rc = CUB_ERR_INVALID;
+  switch (ndim) {
+#define CUB_SPLIT_CASE(N)                                                                      \
+  case N:                                                                                     \
+    rc = split_dim_##N(n, d_lo, d_len, ld, d_active, d_axis, d_out_lo, d_out_len, out_ld,     \
+                       layout, d_count, cnt, excl, s);                                        \
+    break;
+    CUB_SPLIT_CASE(2) CUB_SPLIT_CASE(3) CUB_SPLIT_CASE(4) CUB_SPLIT_CASE(5) CUB_SPLIT_CASE(6)
+    CUB_SPLIT_CASE(7) CUB_SPLIT_CASE(8)
+#undef CUB_SPLIT_CASE
+  }
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "split kernel launch");
+  return rc;
+}
+
+int cub_reduce(long long n, const double* d_avg, const double* d_err, const int* d_active,
+               double* d_out, void* d_scratch, size_t scratch_bytes, void* stream) {
+  if (n < 0 || !d_out || scratch_bytes < cub_reduce_scratch_bytes(n) || !d_scratch ||
+      (n > 0 && (!d_avg || !d_err || !d_active))) {
+    set_error("invalid argument");
+    return CUB_ERR_INVALID;
+  }
+  const cudaStream_t s = as_stream(stream);
+  double* part = static_cast<double*>(d_scratch);
+  const long long want = (n + 255) / 256;
+  const int blocks = (int)std::max<long long>(1, std::min<long long>(want, kReduceBlocks));
+  k_step_reduce<<<blocks, 256, 0, s>>>(n, d_avg, d_err, d_active, part);
+  k_step_reduce_final<<<1, 32, 0, s>>>(blocks, part, d_out);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "reduce kernel launch");
+  return 0;
+}
+
+}  // extern "C"

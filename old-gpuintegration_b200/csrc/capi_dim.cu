@@ -1,0 +1,102 @@
+// capi_dim.cu -- instantiations of the engine for one dimension (compiled
+// once per dimension with -DCUB_DIM=N) and the built-in integrand families.
+#include "capi_internal.h"
+#include "cubature/step_kernels.cuh"
+
+#ifndef CUB_DIM
+#error "compile with -DCUB_DIM=<ndim>"
+#endif
+
+#define CUB_CAT2(a, b) a##b
+#define CUB_CAT(a, b) CUB_CAT2(a, b)
+
+namespace cubature {
+namespace capi {
+namespace {
+
+constexpr int N = CUB_DIM;
+
+template <template <int> class Fam>
+int run_family(cub_ctx* ctx, int count, const GenzParams* h_params, const GenzParams* d_params,
+               const double* epsrel, const double* epsabs, const Options& opt, Result* out) {
+  if (count == 1) {
+    detail::SingleSource<Fam<N>> src{Fam<N>::load(h_params[0])};
+    return run_batch<N>(*ctx->ws, src, 1, epsrel, epsabs, opt, out, ctx->stream);
+  }
+  detail::ParamSource<Fam<N>> src{d_params};
+  return run_batch<N>(*ctx->ws, src, count, epsrel, epsabs, opt, out, ctx->stream);
+}
+
+template <template <int> class Fam>
+int rule_family(const GenzParams& p, long long n, const double* lo, const double* len,
+                long long ld, double epsrel, double epsabs, double* avg, double* err, int* axis,
+                int* active, cudaStream_t s) {
+  const RuleTables T = make_rule9_tables(N);
+  const Fam<N> f = Fam<N>::load(p);
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const int sms = sm_count(dev);
+  if (n >= (long long)sms * 512) {
+    const long long blocks = std::min<long long>((n + 255) / 256, (long long)sms * 32);
+    k_step_rule<N, 1><<<(unsigned)blocks, 256, 0, s>>>(f, T, n, lo, len, ld, epsrel, epsabs, avg,
+                                                       err, axis, active);
+  } else {
+    const long long blocks = std::max<long long>(1, (n * 32 + 255) / 256);
+    k_step_rule<N, 32><<<(unsigned)std::min<long long>(blocks, (long long)sms * 32), 256, 0, s>>>(
+        f, T, n, lo, len, ld, epsrel, epsabs, avg, err, axis, active);
+  }
+  return 0;
+}
+
+}  // namespace
+
+int CUB_CAT(run_dim_, CUB_DIM)(cub_ctx* ctx, int family, int count, const GenzParams* h_params,
+                               const GenzParams* d_params, const double* epsrel,
+                               const double* epsabs, const Options& opt, Result* out) {
+  switch (family) {
+    case kGaussian: return run_family<Gaussian>(ctx, count, h_params, d_params, epsrel, epsabs, opt, out);
+    case kOscillatory: return run_family<Oscillatory>(ctx, count, h_params, d_params, epsrel, epsabs, opt, out);
+    case kCornerPeak: return run_family<CornerPeak>(ctx, count, h_params, d_params, epsrel, epsabs, opt, out);
+    case kProductPeak: return run_family<ProductPeak>(ctx, count, h_params, d_params, epsrel, epsabs, opt, out);
+    case kContinuous: return run_family<Continuous>(ctx, count, h_params, d_params, epsrel, epsabs, opt, out);
+    case kDiscontinuous: return run_family<Discontinuous>(ctx, count, h_params, d_params, epsrel, epsabs, opt, out);
+    case kCosSum: return run_family<CosSum>(ctx, count, h_params, d_params, epsrel, epsabs, opt, out);
+  }
+  return CUB_ERR_INVALID;
+}
+
+int CUB_CAT(rule_eval_dim_, CUB_DIM)(int family, const GenzParams& p, long long n,
+                                     const double* lo, const double* len, long long ld,
+                                     double epsrel, double epsabs, double* avg, double* err,
+                                     int* axis, int* active, cudaStream_t s) {
+  switch (family) {
+    case kGaussian: return rule_family<Gaussian>(p, n, lo, len, ld, epsrel, epsabs, avg, err, axis, active, s);
+    case kOscillatory: return rule_family<Oscillatory>(p, n, lo, len, ld, epsrel, epsabs, avg, err, axis, active, s);
+    case kCornerPeak: return rule_family<CornerPeak>(p, n, lo, len, ld, epsrel, epsabs, avg, err, axis, active, s);
+    case kProductPeak: return rule_family<ProductPeak>(p, n, lo, len, ld, epsrel, epsabs, avg, err, axis, active, s);
+    case kContinuous: return rule_family<Continuous>(p, n, lo, len, ld, epsrel, epsabs, avg, err, axis, active, s);
+    case kDiscontinuous: return rule_family<Discontinuous>(p, n, lo, len, ld, epsrel, epsabs, avg, err, axis, active, s);
+    case kCosSum: return rule_family<CosSum>(p, n, lo, len, ld, epsrel, epsabs, avg, err, axis, active, s);
+  }
+  return CUB_ERR_INVALID;
+}
+
+int CUB_CAT(split_dim_, CUB_DIM)(long long n, const double* lo, const double* len, long long ld,
+                                 const int* active, const int* axis, double* olo, double* olen,
+                                 long long old, int layout, long long* count, int* cnt,
+                                 int* excl, cudaStream_t s) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const int sms = sm_count(dev);
+  const long long nchunk = (n + 31) / 32;
+  const unsigned blocks =
+      (unsigned)std::max<long long>(1, std::min<long long>((nchunk + 7) / 8, (long long)sms * 16));
+  k_step_count<<<blocks, 256, 0, s>>>(n, active, cnt);
+  k_step_scan<<<1, 1024, 0, s>>>(nchunk, cnt, excl, count);
+  k_step_write<N><<<blocks, 256, 0, s>>>(n, lo, len, ld, active, axis, excl, count, olo, olen,
+                                         old, layout);
+  return 0;
+}
+
+}  // namespace capi
+}  // namespace cubature

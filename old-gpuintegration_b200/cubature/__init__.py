@@ -1,0 +1,427 @@
+"""Python front end of the B200 adaptive cubature engine.
+
+Thin ctypes layer over the C ABI in include/cubature.h
+(libcubature_b200.so, built in-tree by old-gpuintegration_b200/build.py).
+It mirrors the reference's public API, quad::GPUcuhre<T>
+(quad/GPUquad/GPUquad.h:46-63 constructor, :611-727 integrate), for the
+built-in integrand families, plus batched integration and the per-step
+entry points.  There is no CPU fallback: if the CUDA library is missing or
+no GPU is present the calls raise.
+
+PyTorch is used only as a device-memory container for the per-step entry
+points (tensors are passed to the library as raw device pointers).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass
+from pathlib import Path
+from typing import Iterable, Sequence
+
+LIB_PATH = Path(__file__).resolve().parent / "libcubature_b200.so"
+
+MAXDIM = 16
+MIN_NDIM = 2
+MAX_NDIM = 8
+
+GAUSSIAN, OSCILLATORY, CORNER_PEAK, PRODUCT_PEAK, CONTINUOUS, DISCONTINUOUS, COSSUM = range(1, 8)
+FAMILIES = {
+    "gaussian": GAUSSIAN,
+    "oscillatory": OSCILLATORY,
+    "corner_peak": CORNER_PEAK,
+    "product_peak": PRODUCT_PEAK,
+    "continuous": CONTINUOUS,
+    "discontinuous": DISCONTINUOUS,
+    "cossum": COSSUM,
+}
+
+POLICY_REFERENCE = 0
+POLICY_BREADTH = 1
+
+ERR_INVALID, ERR_CUDA, ERR_CAPACITY, ERR_UNSUPPORTED = -1, -2, -3, -4
+
+
+class CubatureError(RuntimeError):
+    """An API or CUDA error reported by the library."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"[{code}] {message}")
+        self.code = code
+
+
+class GenzParams(C.Structure):
+    _fields_ = [("a", C.c_double * MAXDIM), ("u", C.c_double * MAXDIM)]
+
+
+class CResult(C.Structure):
+    _fields_ = [
+        ("value", C.c_double),
+        ("error", C.c_double),
+        ("nregions", C.c_ulonglong),
+        ("neval", C.c_ulonglong),
+        ("status", C.c_int),
+        ("iterations", C.c_int),
+        ("state", C.c_int),
+        ("reserved", C.c_int),
+    ]
+
+
+class CStats(C.Structure):
+    _fields_ = [
+        ("ms_eval", C.c_double),
+        ("ms_phase2", C.c_double),
+        ("eval_launches", C.c_longlong),
+        ("launches", C.c_longlong),
+        ("regions_evaluated", C.c_longlong),
+        ("iterations", C.c_longlong),
+        ("phase2_boxes", C.c_longlong),
+        ("h2d_bytes", C.c_longlong),
+        ("d2h_bytes", C.c_longlong),
+    ]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class COptions(C.Structure):
+    _fields_ = [
+        ("policy", C.c_int),
+        ("phase1_cap", C.c_int),
+        ("max_iters", C.c_int),
+        ("phase2_max_regions", C.c_int),
+        ("max_slots", C.c_longlong),
+        ("lanes", C.c_int),
+        ("reserved", C.c_int),
+    ]
+
+
+#: every symbol include/cubature.h declares
+EXPORTS = (
+    "cub_version", "cub_last_error", "cub_default_options", "cub_create", "cub_destroy",
+    "cub_ctx_bytes", "cub_integrate", "cub_integrate_batch", "cub_rule_tables", "cub_rule_eval",
+    "cub_split_scratch_bytes", "cub_reduce_scratch_bytes", "cub_split", "cub_reduce",
+    "cub_ctx_stream", "cub_ctx_stats", "cub_ctx_reset_stats", "cub_ctx_set_timing",
+)
+
+_lib = None
+
+
+def load_library(path: str | Path | None = None):
+    """Load libcubature_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise ImportError(f"{p} is missing: build it with old-gpuintegration_b200/build.py")
+    L = C.CDLL(str(p))
+    vp, dp, ip = C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int)
+    L.cub_version.restype = C.c_int
+    L.cub_last_error.restype = C.c_char_p
+    L.cub_default_options.argtypes = [C.POINTER(COptions)]
+    L.cub_create.restype = vp
+    L.cub_create.argtypes = [C.c_int]
+    L.cub_destroy.argtypes = [vp]
+    L.cub_ctx_bytes.argtypes = [vp]
+    L.cub_ctx_bytes.restype = C.c_size_t
+    L.cub_integrate.argtypes = [vp, C.c_int, C.c_int, C.POINTER(GenzParams), C.c_double,
+                                C.c_double, C.POINTER(COptions), C.POINTER(CResult)]
+    L.cub_integrate_batch.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.POINTER(GenzParams), dp, dp,
+                                      C.c_double, C.c_double, C.POINTER(COptions),
+                                      C.POINTER(CResult)]
+    L.cub_ctx_stream.argtypes = [vp]
+    L.cub_ctx_stream.restype = vp
+    L.cub_ctx_stats.argtypes = [vp, C.POINTER(CStats)]
+    L.cub_ctx_reset_stats.argtypes = [vp]
+    L.cub_ctx_set_timing.argtypes = [vp, C.c_int]
+    L.cub_rule_tables.argtypes = [C.c_int, dp, dp, dp, ip]
+    L.cub_rule_eval.argtypes = [C.c_int, C.c_int, C.POINTER(GenzParams), C.c_longlong, vp, vp,
+                                C.c_longlong, C.c_double, C.c_double, vp, vp, vp, vp, vp]
+    L.cub_split_scratch_bytes.argtypes = [C.c_longlong]
+    L.cub_split_scratch_bytes.restype = C.c_size_t
+    L.cub_reduce_scratch_bytes.argtypes = [C.c_longlong]
+    L.cub_reduce_scratch_bytes.restype = C.c_size_t
+    L.cub_split.argtypes = [C.c_int, C.c_longlong, vp, vp, C.c_longlong, vp, vp, vp, vp,
+                            C.c_longlong, C.c_int, vp, vp, C.c_size_t, vp]
+    L.cub_reduce.argtypes = [C.c_longlong, vp, vp, vp, vp, vp, C.c_size_t, vp]
+    if path is None:
+        _lib = L
+    return L
+
+
+def last_error() -> str:
+    return load_library().cub_last_error().decode()
+
+
+def _check(rc: int) -> int:
+    if rc < 0:
+        raise CubatureError(rc, last_error())
+    return rc
+
+
+def family_id(family) -> int:
+    if isinstance(family, str):
+        return FAMILIES[family]
+    return int(family)
+
+
+def make_params(ndim: int, a=1.0, u=0.5) -> GenzParams:
+    p = GenzParams()
+    a = _vec(a, ndim)
+    u = _vec(u, ndim)
+    for d in range(ndim):
+        p.a[d] = a[d]
+        p.u[d] = u[d]
+    return p
+
+
+def _vec(v, n) -> list[float]:
+    if isinstance(v, (int, float)):
+        return [float(v)] * n
+    v = [float(x) for x in v]
+    if len(v) != n:
+        raise ValueError(f"expected {n} values, got {len(v)}")
+    return v
+
+
+@dataclass
+class Integrand:
+    """A built-in integrand family with its parameters (device functor id)."""
+
+    family: int | str
+    ndim: int
+    a: float | Sequence[float] = 1.0
+    u: float | Sequence[float] = 0.5
+
+    def params(self) -> GenzParams:
+        return make_params(self.ndim, self.a, self.u)
+
+
+@dataclass
+class Result:
+    integral: float
+    error: float
+    nregions: int
+    neval: int
+    status: int  # the reference's errorFlag: 0 = converged
+    iterations: int
+    state: int
+
+    @property
+    def errorFlag(self) -> int:  # noqa: N802 - reference spelling
+        return self.status
+
+    @staticmethod
+    def from_c(r: CResult) -> "Result":
+        return Result(r.value, r.error, int(r.nregions), int(r.neval), r.status, r.iterations,
+                      r.state)
+
+
+def options(policy: int = POLICY_REFERENCE, phase1_cap: int = 0, max_iters: int = 0,
+            phase2_max_regions: int = 0, max_slots: int = 0, lanes: int = 0) -> COptions:
+    o = COptions()
+    load_library().cub_default_options(C.byref(o))
+    o.policy = policy
+    if phase1_cap:
+        o.phase1_cap = phase1_cap
+    if max_iters:
+        o.max_iters = max_iters
+    if phase2_max_regions:
+        o.phase2_max_regions = phase2_max_regions
+    if max_slots:
+        o.max_slots = max_slots
+    o.lanes = lanes
+    return o
+
+
+class Context:
+    """A device context (stream + pooled device memory)."""
+
+    def __init__(self, device: int = 0):
+        self._lib = load_library()
+        h = self._lib.cub_create(device)
+        if not h:
+            raise CubatureError(ERR_CUDA, last_error())
+        self._h = h
+        self.device = device
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.cub_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def bytes_reserved(self) -> int:
+        return int(self._lib.cub_ctx_bytes(self._h))
+
+    @property
+    def stream(self) -> int:
+        """The context's cudaStream_t as an integer handle."""
+        return int(self._lib.cub_ctx_stream(self._h) or 0)
+
+    def stats(self) -> dict:
+        st = CStats()
+        _check(self._lib.cub_ctx_stats(self._h, C.byref(st)))
+        return st.as_dict()
+
+    def reset_stats(self):
+        self._lib.cub_ctx_reset_stats(self._h)
+
+    def set_timing(self, on: bool):
+        self._lib.cub_ctx_set_timing(self._h, 1 if on else 0)
+
+    def integrate(self, f: Integrand, epsrel: float, epsabs: float,
+                  opts: COptions | None = None) -> Result:
+        out = CResult()
+        p = f.params()
+        _check(self._lib.cub_integrate(self._h, family_id(f.family), f.ndim, C.byref(p), epsrel,
+                                       epsabs, C.byref(opts) if opts else None, C.byref(out)))
+        return Result.from_c(out)
+
+    def integrate_batch(self, family, ndim: int, params: Sequence[GenzParams], epsrel,
+                        epsabs, opts: COptions | None = None) -> list[Result]:
+        n = len(params)
+        arr = (GenzParams * n)(*params)
+        out = (CResult * n)()
+        er = ea = None
+        er0 = ea0 = 0.0
+        if isinstance(epsrel, (int, float)):
+            er0 = float(epsrel)
+        else:
+            er = (C.c_double * n)(*[float(x) for x in epsrel])
+        if isinstance(epsabs, (int, float)):
+            ea0 = float(epsabs)
+        else:
+            ea = (C.c_double * n)(*[float(x) for x in epsabs])
+        rc = self._lib.cub_integrate_batch(self._h, family_id(family), ndim, n, arr, er, ea, er0,
+                                           ea0, C.byref(opts) if opts else None, out)
+        if rc < 0 and rc != ERR_CAPACITY:
+            raise CubatureError(rc, last_error())
+        return [Result.from_c(out[i]) for i in range(n)]
+
+
+class GPUcuhre:
+    """Mirror of quad::GPUcuhre<double> (GPUquad.h:26-727) for built-in
+    integrands: GPUcuhre(ndim, key, verbose, numDevices).integrate(...).
+
+    The reference resets every visible device in its constructor and
+    accumulates into the caller's integral/error/nregions/neval; this class
+    does neither: integrate() returns a fresh Result.
+    """
+
+    def __init__(self, ndim: int, key: int = 0, verbose: int = 0, num_devices: int = 1,
+                 device: int = 0):
+        if not MIN_NDIM <= ndim <= MAX_NDIM:
+            raise ValueError(f"ndim must be in [{MIN_NDIM}, {MAX_NDIM}]")
+        if key not in (0, 9):
+            raise ValueError("only the degree-9 rule (key 0 or 9) is implemented")
+        self.ndim = ndim
+        self.key = key
+        self.verbose = verbose
+        self.num_devices = num_devices
+        self.ctx = Context(device)
+
+    def integrate(self, f: Integrand, epsrel: float, epsabs: float,
+                  policy: int = POLICY_REFERENCE, **kw) -> Result:
+        if f.ndim != self.ndim:
+            raise ValueError("integrand dimension does not match the rule")
+        return self.ctx.integrate(f, epsrel, epsabs, options(policy=policy, **kw))
+
+
+def rule_tables(ndim: int):
+    import numpy as np
+
+    wt = np.zeros(45)
+    sc = np.zeros(45)
+    nm = np.zeros(45)
+    cnt = np.zeros(9, dtype=np.int32)
+    dp = C.POINTER(C.c_double)
+    _check(load_library().cub_rule_tables(ndim, wt.ctypes.data_as(dp), sc.ctypes.data_as(dp),
+                                          nm.ctypes.data_as(dp),
+                                          cnt.ctypes.data_as(C.POINTER(C.c_int))))
+    return {"wt": wt.reshape(9, 5), "scale": sc.reshape(9, 5), "norm": nm.reshape(9, 5),
+            "count": cnt}
+
+
+def npoints(ndim: int) -> int:
+    return 1 + 8 * ndim + 6 * ndim * (ndim - 1) + 4 * ndim * (ndim - 1) * (ndim - 2) // 3 + (1 << ndim)
+
+
+# ---- per-step entry points on torch CUDA tensors ---------------------------
+
+def _ptr(t) -> int:
+    return t.data_ptr()
+
+
+def _stream_ptr(stream) -> int | None:
+    if stream is None:
+        import torch
+        return torch.cuda.current_stream().cuda_stream
+    return stream
+
+
+def rule_eval(f: Integrand, lo, length, epsrel: float, epsabs: float, stream=None):
+    """Phase-1 rule + classification on a [ndim][n] SoA region list of FP64
+    CUDA tensors.  Returns (avg, err, axis, active) CUDA tensors."""
+    import torch
+
+    ndim, n = lo.shape
+    assert lo.is_cuda and lo.dtype == torch.float64 and lo.is_contiguous()
+    assert length.shape == lo.shape and length.is_contiguous()
+    avg = torch.empty(n, dtype=torch.float64, device=lo.device)
+    err = torch.empty_like(avg)
+    axis = torch.empty(n, dtype=torch.int32, device=lo.device)
+    act = torch.empty_like(axis)
+    p = f.params()
+    _check(load_library().cub_rule_eval(family_id(f.family), ndim, C.byref(p), n, _ptr(lo),
+                                        _ptr(length), n, epsrel, epsabs, _ptr(avg), _ptr(err),
+                                        _ptr(axis), _ptr(act), _stream_ptr(stream)))
+    return avg, err, axis, act
+
+
+def split(lo, length, active, axis, layout: int = 0, stream=None):
+    """Scan + compact + bisect; returns (children_lo, children_len) [ndim][2m]."""
+    import torch
+
+    ndim, n = lo.shape
+    L = load_library()
+    dev = lo.device
+    scratch = torch.empty(max(1, L.cub_split_scratch_bytes(n)), dtype=torch.uint8, device=dev)
+    count = torch.zeros(1, dtype=torch.int64, device=dev)
+    cap = max(2 * int(active.sum().item()), 1)
+    olo = torch.empty((ndim, cap), dtype=torch.float64, device=dev)
+    olen = torch.empty_like(olo)
+    _check(L.cub_split(ndim, n, _ptr(lo), _ptr(length), n, _ptr(active), _ptr(axis), _ptr(olo),
+                       _ptr(olen), cap, layout, _ptr(count), _ptr(scratch), scratch.numel(),
+                       _stream_ptr(stream)))
+    m2 = int(count.item())
+    return olo[:, :m2].contiguous(), olen[:, :m2].contiguous()
+
+
+def reduce(avg, err, active, stream=None):
+    """The four phase-1 sums: [sum avg, sum err, finished avg, finished err]."""
+    import torch
+
+    n = avg.numel()
+    L = load_library()
+    scratch = torch.empty(L.cub_reduce_scratch_bytes(n), dtype=torch.uint8, device=avg.device)
+    out = torch.empty(4, dtype=torch.float64, device=avg.device)
+    _check(L.cub_reduce(n, _ptr(avg), _ptr(err), _ptr(active), _ptr(out), _ptr(scratch),
+                        scratch.numel(), _stream_ptr(stream)))
+    return out

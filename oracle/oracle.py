@@ -1,0 +1,264 @@
+"""ctypes bindings for the CPU oracle (oracle/cuhre_oracle.c).
+
+TEST INFRASTRUCTURE ONLY: loaded by tests/, __graft_entry__.smoke() and the
+CPU legs of bench.py as the checker and the CPU baseline.  The product
+library never imports this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "_build" / "libcuhre_oracle.so"
+
+MAXDIM = 16
+GAUSSIAN, OSCILLATORY, CORNER_PEAK, PRODUCT_PEAK, CONTINUOUS, DISCONTINUOUS, COSSUM = range(1, 8)
+FAMILY_NAMES = {
+    "gaussian": GAUSSIAN,
+    "oscillatory": OSCILLATORY,
+    "corner_peak": CORNER_PEAK,
+    "product_peak": PRODUCT_PEAK,
+    "continuous": CONTINUOUS,
+    "discontinuous": DISCONTINUOUS,
+    "cossum": COSSUM,
+}
+
+
+class Integrand(C.Structure):
+    _fields_ = [
+        ("family", C.c_int),
+        ("ndim", C.c_int),
+        ("a", C.c_double * MAXDIM),
+        ("u", C.c_double * MAXDIM),
+    ]
+
+
+class Result(C.Structure):
+    _fields_ = [("avg", C.c_double), ("err", C.c_double), ("axis", C.c_int), ("axis_margin", C.c_double)]
+
+
+class Out(C.Structure):
+    _fields_ = [
+        ("value", C.c_double),
+        ("error", C.c_double),
+        ("nregions", C.c_size_t),
+        ("neval", C.c_size_t),
+        ("status", C.c_int),
+        ("phase1_iters", C.c_int),
+        ("phase2_regions", C.c_size_t),
+        ("phase2_failed", C.c_size_t),
+    ]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+def build() -> Path:
+    """Compile the oracle with its Makefile (idempotent)."""
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    return LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            build()
+        L = C.CDLL(str(LIB_PATH))
+        dp = C.POINTER(C.c_double)
+        ip = C.POINTER(C.c_int)
+        L.orc_rule_new.restype = C.c_void_p
+        L.orc_rule_new.argtypes = [C.c_int]
+        L.orc_rule_free.argtypes = [C.c_void_p]
+        L.orc_rule_npoints.argtypes = [C.c_void_p]
+        L.orc_rule_npoints.restype = C.c_int
+        L.orc_rule_tables.argtypes = [C.c_void_p, dp, dp, dp, dp, ip]
+        L.orc_rule_points.argtypes = [C.c_void_p, dp, ip]
+        L.orc_npoints_formula.argtypes = [C.c_int]
+        L.orc_npoints_formula.restype = C.c_int
+        L.orc_eval_integrand.argtypes = [C.POINTER(Integrand), dp]
+        L.orc_eval_integrand.restype = C.c_double
+        L.orc_exact.argtypes = [C.POINTER(Integrand)]
+        L.orc_exact.restype = C.c_double
+        L.orc_eval_region.argtypes = [C.c_void_p, C.POINTER(Integrand), dp, dp, dp, dp, C.c_int,
+                                      C.POINTER(Result)]
+        L.orc_phase1_eval.argtypes = [C.c_void_p, C.POINTER(Integrand), C.c_size_t, dp, dp,
+                                      C.c_double, C.c_double, dp, dp, ip, ip, dp, dp, C.c_int]
+        L.orc_split.argtypes = [C.c_int, C.c_size_t, dp, dp, ip, ip, dp, dp]
+        L.orc_split.restype = C.c_size_t
+        L.orc_initial_grid.argtypes = [C.c_int, dp, dp]
+        L.orc_initial_grid.restype = C.c_size_t
+        L.orc_phase2_box.argtypes = [C.c_void_p, C.POINTER(Integrand), dp, dp, C.c_double,
+                                     C.c_double, C.c_int, dp, dp, ip]
+        L.orc_phase2_box.restype = C.c_int
+        L.orc_integrate_reference.argtypes = [C.c_void_p, C.POINTER(Integrand), C.c_double,
+                                              C.c_double, C.c_int, C.c_int, C.c_int,
+                                              C.POINTER(Out)]
+        L.orc_integrate_global.argtypes = [C.c_void_p, C.POINTER(Integrand), C.c_double,
+                                           C.c_double, C.c_size_t, C.c_int, C.c_int,
+                                           C.POINTER(Out)]
+        L.orc_cuhre_sequential.argtypes = [C.c_void_p, C.POINTER(Integrand), C.c_double,
+                                           C.c_double, C.c_size_t, C.POINTER(Out)]
+        L.orc_max_threads.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _ip(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+def make_integrand(family, ndim: int, a, u) -> Integrand:
+    fam = FAMILY_NAMES[family] if isinstance(family, str) else int(family)
+    f = Integrand()
+    f.family = fam
+    f.ndim = ndim
+    a = np.broadcast_to(np.asarray(a, dtype=np.float64), (ndim,))
+    u = np.broadcast_to(np.asarray(u, dtype=np.float64), (ndim,))
+    for d in range(ndim):
+        f.a[d] = float(a[d])
+        f.u[d] = float(u[d])
+    return f
+
+
+class Rule:
+    """The degree-9 rule for one dimension (GPUQuadRule.cu:31-390)."""
+
+    def __init__(self, ndim: int):
+        self.ndim = ndim
+        self._h = lib().orc_rule_new(ndim)
+        if not self._h:
+            raise ValueError(f"ndim {ndim} out of range")
+        self.npoints = lib().orc_rule_npoints(self._h)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and _lib is not None:
+            _lib.orc_rule_free(h)
+            self._h = None
+
+    def tables(self):
+        n = self.ndim
+        gen = np.zeros(9 * n)
+        wt = np.zeros(45)
+        sc = np.zeros(45)
+        nm = np.zeros(45)
+        cnt = np.zeros(9, dtype=np.int32)
+        lib().orc_rule_tables(self._h, _dp(gen), _dp(wt), _dp(sc), _dp(nm), _ip(cnt))
+        return {"gen": gen.reshape(9, n), "wt": wt.reshape(9, 5), "scale": sc.reshape(9, 5),
+                "norm": nm.reshape(9, 5), "count": cnt}
+
+    def points(self):
+        g = np.zeros(self.npoints * self.ndim)
+        s = np.zeros(self.npoints, dtype=np.int32)
+        lib().orc_rule_points(self._h, _dp(g), _ip(s))
+        return g.reshape(self.npoints, self.ndim), s
+
+    # -- per-region and per-step checkers --------------------------------
+    def eval_region(self, f: Integrand, L, W, llo=None, lhi=None, div=0):
+        L = np.ascontiguousarray(L, dtype=np.float64)
+        W = np.ascontiguousarray(W, dtype=np.float64)
+        res = Result()
+        lo_p = _dp(np.ascontiguousarray(llo, dtype=np.float64)) if llo is not None else None
+        hi_p = _dp(np.ascontiguousarray(lhi, dtype=np.float64)) if lhi is not None else None
+        lib().orc_eval_region(self._h, C.byref(f), _dp(L), _dp(W), lo_p, hi_p, div, C.byref(res))
+        return res.avg, res.err, res.axis, res.axis_margin
+
+    def phase1_eval(self, f: Integrand, lo, length, epsrel, epsabs, nthreads=0):
+        lo = np.ascontiguousarray(lo, dtype=np.float64)
+        length = np.ascontiguousarray(length, dtype=np.float64)
+        n = lo.shape[1]
+        avg = np.zeros(n)
+        err = np.zeros(n)
+        axis = np.zeros(n, dtype=np.int32)
+        act = np.zeros(n, dtype=np.int32)
+        margin = np.zeros(n)
+        ratio = np.zeros(n)
+        lib().orc_phase1_eval(self._h, C.byref(f), n, _dp(lo), _dp(length), epsrel, epsabs,
+                              _dp(avg), _dp(err), _ip(axis), _ip(act), _dp(margin), _dp(ratio),
+                              nthreads)
+        return {"avg": avg, "err": err, "axis": axis, "active": act, "margin": margin,
+                "ratio": ratio}
+
+    def integrate_reference(self, f: Integrand, epsrel, epsabs, phase1_cap=0, phase2_max=0,
+                            nthreads=0):
+        out = Out()
+        lib().orc_integrate_reference(self._h, C.byref(f), epsrel, epsabs, phase1_cap, phase2_max,
+                                      nthreads, C.byref(out))
+        return out.as_dict()
+
+    def integrate_global(self, f: Integrand, epsrel, epsabs, max_regions=1 << 26, max_iters=200,
+                         nthreads=0):
+        out = Out()
+        lib().orc_integrate_global(self._h, C.byref(f), epsrel, epsabs, max_regions, max_iters,
+                                   nthreads, C.byref(out))
+        return out.as_dict()
+
+    def cuhre_sequential(self, f: Integrand, epsrel, epsabs, max_regions=1 << 22):
+        out = Out()
+        lib().orc_cuhre_sequential(self._h, C.byref(f), epsrel, epsabs, max_regions, C.byref(out))
+        return out.as_dict()
+
+    def phase2_box(self, f: Integrand, L, W, epsrel, epsabs, max_regions=2048):
+        L = np.ascontiguousarray(L, dtype=np.float64)
+        W = np.ascontiguousarray(W, dtype=np.float64)
+        res = C.c_double()
+        err = C.c_double()
+        fail = C.c_int()
+        n = lib().orc_phase2_box(self._h, C.byref(f), _dp(L), _dp(W), epsrel, epsabs, max_regions,
+                                 C.byref(res), C.byref(err), C.byref(fail))
+        return res.value, err.value, n, fail.value
+
+
+def npoints(ndim: int) -> int:
+    return lib().orc_npoints_formula(ndim)
+
+
+def exact(f: Integrand) -> float:
+    return lib().orc_exact(C.byref(f))
+
+
+def eval_integrand(f: Integrand, x) -> float:
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    return lib().orc_eval_integrand(C.byref(f), _dp(x))
+
+
+def initial_grid(ndim: int):
+    n = lib().orc_initial_grid(ndim, None, None)
+    lo = np.zeros((ndim, n))
+    ln = np.zeros((ndim, n))
+    lib().orc_initial_grid(ndim, _dp(lo), _dp(ln))
+    return lo, ln
+
+
+def split(lo, length, active, axis):
+    lo = np.ascontiguousarray(lo, dtype=np.float64)
+    length = np.ascontiguousarray(length, dtype=np.float64)
+    active = np.ascontiguousarray(active, dtype=np.int32)
+    axis = np.ascontiguousarray(axis, dtype=np.int32)
+    ndim, n = lo.shape
+    m = int((active == 1).sum())
+    olo = np.zeros((ndim, max(2 * m, 1)))
+    oln = np.zeros((ndim, max(2 * m, 1)))
+    k = lib().orc_split(ndim, n, _dp(lo), _dp(length), _ip(active), _ip(axis), _dp(olo), _dp(oln))
+    return olo[:, :k], oln[:, :k]
+
+
+def max_threads() -> int:
+    return lib().orc_max_threads()
+
+
+os.environ.setdefault("OMP_PROC_BIND", "false")

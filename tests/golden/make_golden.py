@@ -1,0 +1,170 @@
+"""Generate golden vectors from the reference engine itself.
+
+Runs oracle/_ref/ref_driver -- marcpaterno/old-gpuintegration's quad/
+engine compiled from its own sources by oracle/ref_driver/Makefile -- on a
+CUDA device, and writes:
+
+  ref_integrate.json   GPUcuhre::integrate outputs (integral, error,
+                       nregions, neval, errorFlag) for a list of Genz cases
+  ref_phase1_<name>.npz  INTEGRATE_GPU_PHASE1 per-region outputs (value,
+                       error, active flag, split axis) on deterministic
+                       dyadic region lists, with the inputs
+
+    python tests/golden/make_golden.py --out <dir>
+
+The reference resets every visible device when it starts
+(quad/util/cudaUtil.h:151-161), so run this with one GPU visible.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+DRIVER = ROOT / "oracle" / "_ref" / "ref_driver"
+FAMILY = {"gaussian": 1, "oscillatory": 2, "corner_peak": 3, "product_peak": 4,
+          "continuous": 5, "discontinuous": 6, "cossum": 7}
+
+
+def product_peak_params(n, seed):
+    rng = np.random.default_rng(seed)
+    return (list(np.exp(rng.uniform(0, np.log(50), n))), list(rng.uniform(0.1, 0.9, n)))
+
+
+INTEGRATE_CASES = [
+    ("config1_gaussian5", "gaussian", 5, [5.0] * 5, [0.5] * 5, 1e-3, 1e-12),
+    ("config2_oscillatory8", "oscillatory", 8, [1.1] * 8, [0.3] * 8, 1e-6, 1e-12),
+    ("config2_cornerpeak8", "corner_peak", 8, [0.5] * 8, [0.0] * 8, 1e-6, 1e-12),
+    ("gaussian3", "gaussian", 3, [4.0, 6.0, 5.0], [0.3, 0.5, 0.6], 1e-7, 1e-12),
+    ("productpeak4", "product_peak", 4, [8.0, 12.0, 6.0, 10.0], [0.3, 0.6, 0.5, 0.4], 1e-5,
+     1e-12),
+    ("continuous2", "continuous", 2, [3.0, 4.0], [0.4, 0.6], 1e-5, 1e-12),
+    ("cossum6", "cossum", 6, [1.0] * 6, [0.0] * 6, 1e-4, 1e-12),
+    ("cornerpeak6_epsabs", "corner_peak", 6, [2.0, 3.0, 2.0, 3.0, 2.0, 3.0], [0.0] * 6, 1e-7,
+     1e-12),
+    ("productpeak4_phase2", "product_peak", 4, [30.0, 40.0, 20.0, 35.0], [0.3, 0.6, 0.5, 0.4],
+     1e-7, 1e-12),
+    ("productpeak5_phase2_failed", "product_peak", 5, [20.0, 30.0, 10.0, 25.0, 15.0],
+     [0.3, 0.5, 0.7, 0.45, 0.6], 1e-7, 1e-12),
+]
+for s in range(4):
+    a, u = product_peak_params(6, s)
+    INTEGRATE_CASES.append((f"config3_productpeak6_seed{s}", "product_peak", 6, a, u, 1e-5,
+                            1e-12))
+
+
+def initial_grid(n):
+    d = 4 if n <= 4 else 2
+    cnt = d ** n
+    idx = np.arange(cnt)
+    lo = np.zeros((n, cnt))
+    for k in range(n):
+        lo[k] = (idx // d ** k) % d * (1.0 / d)
+    return lo, np.full((n, cnt), 1.0 / d)
+
+
+def refined(n, rounds, seed, frac=0.5):
+    """Deterministic dyadic refinement: split a random subset each round."""
+    rng = np.random.default_rng(seed)
+    lo, ln = initial_grid(n)
+    for _ in range(rounds):
+        m = lo.shape[1]
+        act = rng.uniform(size=m) < frac
+        ax = rng.integers(0, n, size=m)
+        keep_lo, keep_ln = lo[:, ~act], ln[:, ~act]
+        plo, pln, pax = lo[:, act], ln[:, act], ax[act]
+        c0lo, c0ln = plo.copy(), pln.copy()
+        c1lo, c1ln = plo.copy(), pln.copy()
+        j = np.arange(plo.shape[1])
+        c0ln[pax, j] /= 2
+        c1ln[pax, j] /= 2
+        c1lo[pax, j] += c1ln[pax, j]
+        lo = np.concatenate([keep_lo, c0lo, c1lo], axis=1)
+        ln = np.concatenate([keep_ln, c0ln, c1ln], axis=1)
+    return np.ascontiguousarray(lo), np.ascontiguousarray(ln)
+
+
+PHASE1_CASES = [
+    ("gaussian3", "gaussian", 3, [4.0, 6.0, 5.0], [0.3, 0.5, 0.6], 1e-6, 5),
+    ("oscillatory5", "oscillatory", 5, [1.1, 0.7, 1.5, 0.9, 1.3], [0.3] * 5, 1e-6, 3),
+    ("cornerpeak8", "corner_peak", 8, [0.5] * 8, [0.0] * 8, 1e-6, 1),
+    ("productpeak6", "product_peak", 6, *product_peak_params(6, 0), 1e-5, 3),
+    ("gaussian8", "gaussian", 8, [3.0] * 8, [0.45] * 8, 1e-4, 1),
+    ("continuous4", "continuous", 4, [2.0, 3.0, 1.0, 4.0], [0.4, 0.5, 0.3, 0.6], 1e-4, 3),
+    ("discontinuous3", "discontinuous", 3, [1.0, 2.0, 0.5], [0.6, 0.4, 0.0], 1e-4, 4),
+]
+
+
+def run_integrate(case):
+    name, fam, n, a, u, er, ea = case
+    args = [str(DRIVER), "integrate", str(FAMILY[fam]), str(n), repr(er), repr(ea),
+            *[repr(float(x)) for x in a], *[repr(float(x)) for x in u]]
+    out = subprocess.run(args, capture_output=True, text=True, timeout=600)
+    if out.returncode != 0:
+        raise RuntimeError(f"{name}: rc={out.returncode}\n{out.stderr[-2000:]}")
+    line = [ln for ln in out.stdout.splitlines() if ln.startswith("RESULT ")][-1]
+    rec = json.loads(line[len("RESULT "):])
+    rec.update({"name": name, "family_name": fam, "a": [float(x) for x in a],
+                "u": [float(x) for x in u]})
+    return rec
+
+
+def run_phase1(case, outdir):
+    name, fam, n, a, u, er, rounds = case
+    lo, ln = refined(n, rounds, seed=len(name))
+    with tempfile.TemporaryDirectory() as td:
+        fin, fout = Path(td) / "in.bin", Path(td) / "out.bin"
+        with open(fin, "wb") as fh:
+            np.array([lo.shape[1]], dtype=np.int64).tofile(fh)
+            lo.tofile(fh)
+            ln.tofile(fh)
+        args = [str(DRIVER), "phase1", str(FAMILY[fam]), str(n), repr(er), repr(1e-12), str(fin),
+                str(fout), *[repr(float(x)) for x in a], *[repr(float(x)) for x in u]]
+        out = subprocess.run(args, capture_output=True, text=True, timeout=600)
+        if out.returncode != 0:
+            raise RuntimeError(f"{name}: rc={out.returncode}\n{out.stderr[-2000:]}")
+        m = lo.shape[1]
+        raw = np.fromfile(fout, dtype=np.uint8)
+        avg = raw[: 8 * m].view(np.float64)
+        err = raw[8 * m: 16 * m].view(np.float64)
+        act = raw[16 * m: 20 * m].view(np.int32)
+        ax = raw[20 * m: 24 * m].view(np.int32)
+    np.savez_compressed(outdir / f"ref_phase1_{name}.npz", lo=lo, len=ln, avg=avg, err=err,
+                        active=act, axis=ax, family=fam, ndim=n, a=np.array(a, float),
+                        u=np.array(u, float), epsrel=er, epsabs=1e-12)
+    return m
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=str(Path(__file__).resolve().parent))
+    ap.add_argument("--only", default="")
+    args = ap.parse_args()
+    outdir = Path(args.out)
+    outdir.mkdir(parents=True, exist_ok=True)
+    if not DRIVER.exists():
+        raise SystemExit(f"{DRIVER} missing: build it with make -C oracle/ref_driver")
+    print("CUDA_VISIBLE_DEVICES =", os.environ.get("CUDA_VISIBLE_DEVICES"), flush=True)
+    if args.only in ("", "phase1"):
+        for case in PHASE1_CASES:
+            m = run_phase1(case, outdir)
+            print("phase1", case[0], m, flush=True)
+    if args.only in ("", "integrate"):
+        recs = []
+        for case in INTEGRATE_CASES:
+            rec = run_integrate(case)
+            recs.append(rec)
+            print("integrate", json.dumps(rec), flush=True)
+        (outdir / "ref_integrate.json").write_text(json.dumps(recs, indent=1) + "\n")
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

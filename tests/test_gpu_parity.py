@@ -1,0 +1,253 @@
+"""GPU parity tests: the CUDA path against the CPU oracle on the same
+inputs, through the C ABI.
+
+Tolerances (FP64 throughout):
+  * region value: |avg_gpu - avg_cpu| <= 1e-13 * |avg_cpu| + 1e-300
+  * region error: |err_gpu - err_cpu| <= 1e-12 * |avg_cpu| + 1e-12 * err_cpu
+    (the null rules difference nearly equal sums, so the error is compared
+    on the scale of the value, not of itself);
+  * split axis and active flag: identical, except regions whose top two
+    fourth differences are within 1e-9 (relative) or whose error ratio is
+    within 1e-8 of 1 -- there the last bit of exp/cos decides;
+  * scan/compact/bisect: bit-exact;
+  * full integrations: |I_gpu - I_cpu| <= 2 epsrel |I| and both within
+    their error estimates of the analytic value; region counts within 2%.
+"""
+import math
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+FAMILY_PARAMS = {
+    "gaussian": (lambda n, r: (r.uniform(2, 8, n), r.uniform(0.2, 0.8, n))),
+    "oscillatory": (lambda n, r: (r.uniform(0.5, 2.0, n), np.full(n, r.uniform()))),
+    "corner_peak": (lambda n, r: (r.uniform(0.2, 1.5, n), np.zeros(n))),
+    "product_peak": (lambda n, r: (np.exp(r.uniform(0, np.log(30), n)), r.uniform(0.1, 0.9, n))),
+    "continuous": (lambda n, r: (r.uniform(1, 5, n), r.uniform(0.2, 0.8, n))),
+    "discontinuous": (lambda n, r: (r.uniform(0.2, 1.0, n), r.uniform(0.3, 0.9, n))),
+    "cossum": (lambda n, r: (np.ones(n), np.zeros(n))),
+}
+
+
+def refined_list(oracle, n, rounds, seed, frac=0.5):
+    """Initial grid plus `rounds` random bisections: dyadic boxes as the
+    engine sees them."""
+    rng = np.random.default_rng(seed)
+    lo, ln = oracle.initial_grid(n)
+    for _ in range(rounds):
+        m = lo.shape[1]
+        act = (rng.uniform(size=m) < frac).astype(np.int32)
+        act[0] = 1
+        ax = rng.integers(0, n, size=m).astype(np.int32)
+        clo, cln = oracle.split(lo, ln, act, ax)
+        keep = act == 0
+        lo = np.concatenate([lo[:, keep], clo], axis=1)
+        ln = np.concatenate([ln[:, keep], cln], axis=1)
+    return np.ascontiguousarray(lo), np.ascontiguousarray(ln)
+
+
+def compare_regions(o, g, label):
+    avg_c, err_c = o["avg"], o["err"]
+    avg_g, err_g, ax_g, act_g = [t.cpu().numpy() for t in g]
+    assert np.all(np.abs(avg_g - avg_c) <= 1e-13 * np.abs(avg_c) + 1e-300), label
+    assert np.all(np.abs(err_g - err_c) <= 1e-12 * np.abs(avg_c) + 1e-12 * err_c + 1e-300), label
+    clear_axis = o["margin"] > 1e-9
+    assert np.array_equal(ax_g[clear_axis], o["axis"][clear_axis]), label
+    clear_ratio = np.abs(o["ratio"] - 1) > 1e-8
+    assert np.array_equal(act_g[clear_ratio], o["active"][clear_ratio]), label
+    return int((~clear_axis).sum()), int((~clear_ratio).sum())
+
+
+@pytest.mark.parametrize("family", sorted(FAMILY_PARAMS))
+@pytest.mark.parametrize("n", [2, 3, 5, 8])
+def test_rule_eval_matches_oracle(cub, oracle, ctx, family, n):
+    rng = np.random.default_rng(hash((family, n)) % 2**32)
+    a, u = FAMILY_PARAMS[family](n, rng)
+    rounds = {2: 6, 3: 5, 5: 4, 8: 2}[n]
+    lo, ln = refined_list(oracle, n, rounds, seed=n)
+    f_c = oracle.make_integrand(family, n, a, u)
+    f_g = cub.Integrand(family, n, list(a), list(u))
+    for eps in (1e-3, 1e-6):
+        o = oracle.Rule(n).phase1_eval(f_c, lo, ln, eps, 1e-12)
+        dlo = torch.from_numpy(lo).cuda()
+        dln = torch.from_numpy(ln).cuda()
+        g = cub.rule_eval(f_g, dlo, dln, eps, 1e-12)
+        torch.cuda.synchronize()
+        compare_regions(o, g, (family, n, eps))
+
+
+@pytest.mark.parametrize("family,n", [("product_peak", 5), ("gaussian", 8), ("oscillatory", 6)])
+def test_rule_eval_large_list(cub, oracle, ctx, family, n):
+    """A list long enough for the thread-per-region kernel (>= 148*512)."""
+    rng = np.random.default_rng(7)
+    a, u = FAMILY_PARAMS[family](n, rng)
+    lo, ln = refined_list(oracle, n, 30 if n == 5 else 24, seed=3, frac=0.15)
+    while lo.shape[1] < 80000:
+        lo = np.concatenate([lo, lo], axis=1)
+        ln = np.concatenate([ln, ln], axis=1)
+    lo, ln = np.ascontiguousarray(lo[:, :80000]), np.ascontiguousarray(ln[:, :80000])
+    f_c = oracle.make_integrand(family, n, a, u)
+    o = oracle.Rule(n).phase1_eval(f_c, lo, ln, 1e-5, 1e-12)
+    g = cub.rule_eval(cub.Integrand(family, n, list(a), list(u)), torch.from_numpy(lo).cuda(),
+                      torch.from_numpy(ln).cuda(), 1e-5, 1e-12)
+    torch.cuda.synchronize()
+    compare_regions(o, g, (family, n))
+
+
+@pytest.mark.parametrize("layout", [0, 1])
+@pytest.mark.parametrize("n", [2, 5, 8])
+def test_split_bit_exact(cub, oracle, ctx, layout, n):
+    rng = np.random.default_rng(n + 10 * layout)
+    lo, ln = refined_list(oracle, n, 3, seed=n)
+    m = lo.shape[1]
+    act = (rng.uniform(size=m) < 0.4).astype(np.int32)
+    ax = rng.integers(0, n, size=m).astype(np.int32)
+    clo, cln = oracle.split(lo, ln, act, ax)
+    glo, gln = cub.split(torch.from_numpy(lo).cuda(), torch.from_numpy(ln).cuda(),
+                         torch.from_numpy(act).cuda(), torch.from_numpy(ax).cuda(), layout=layout)
+    glo, gln = glo.cpu().numpy(), gln.cpu().numpy()
+    k = clo.shape[1] // 2
+    if layout == 1:  # adjacent children -> reference layout
+        order = np.concatenate([np.arange(0, 2 * k, 2), np.arange(1, 2 * k, 2)])
+        glo, gln = glo[:, order], gln[:, order]
+    assert glo.shape == clo.shape
+    assert np.array_equal(glo, clo) and np.array_equal(gln, cln)
+
+
+def test_split_empty_and_all(cub, oracle, ctx):
+    lo, ln = oracle.initial_grid(3)
+    z = np.zeros(lo.shape[1], dtype=np.int32)
+    glo, _ = cub.split(torch.from_numpy(lo).cuda(), torch.from_numpy(ln).cuda(),
+                       torch.from_numpy(z).cuda(), torch.from_numpy(z).cuda())
+    assert glo.shape[1] == 0
+    one = np.ones(lo.shape[1], dtype=np.int32)
+    glo, gln = cub.split(torch.from_numpy(lo).cuda(), torch.from_numpy(ln).cuda(),
+                         torch.from_numpy(one).cuda(), torch.from_numpy(z).cuda())
+    clo, cln = oracle.split(lo, ln, one, z)
+    assert np.array_equal(glo.cpu().numpy(), clo) and np.array_equal(gln.cpu().numpy(), cln)
+
+
+def test_reduce(cub, ctx):
+    rng = np.random.default_rng(0)
+    for n in (1, 31, 1000, 300001):
+        avg = rng.normal(size=n)
+        err = rng.uniform(size=n) * 1e-3
+        act = (rng.uniform(size=n) < 0.3).astype(np.int32)
+        out = cub.reduce(torch.from_numpy(avg).cuda(), torch.from_numpy(err).cuda(),
+                         torch.from_numpy(act).cuda()).cpu().numpy()
+        fin = act == 0
+        ref = [math.fsum(avg), math.fsum(err), math.fsum(avg[fin]), math.fsum(err[fin])]
+        scale = [np.abs(avg).sum(), err.sum(), np.abs(avg).sum(), err.sum()]
+        for q in range(4):
+            assert abs(out[q] - ref[q]) <= 1e-13 * scale[q]
+
+
+CASES = [
+    # (family, ndim, a, u, epsrel) -- configuration 1, configuration 2, others
+    ("gaussian", 5, 5.0, 0.5, 1e-3),
+    ("oscillatory", 8, 1.1, 0.3, 1e-6),
+    ("corner_peak", 8, 0.5, 0.0, 1e-6),
+    ("gaussian", 3, [4.0, 6.0, 5.0], [0.3, 0.5, 0.6], 1e-7),
+    ("product_peak", 4, [8.0, 12.0, 6.0, 10.0], [0.3, 0.6, 0.5, 0.4], 1e-5),
+    ("continuous", 2, [3.0, 4.0], [0.4, 0.6], 1e-5),
+    ("cossum", 6, 1.0, 0.0, 1e-4),
+]
+
+
+def _compare_full(r_g, r_c, exact, epsrel, label, count_tol=0.02):
+    assert r_g.status == r_c["status"], label
+    assert abs(r_g.integral - r_c["value"]) <= 2 * epsrel * abs(r_c["value"]) + 1e-15, label
+    if r_c["status"] == 0:
+        assert abs(r_g.integral - exact) <= max(10 * r_g.error, 2 * epsrel * abs(exact)), label
+    assert abs(r_g.nregions - r_c["nregions"]) <= count_tol * r_c["nregions"] + 4, label
+    assert r_g.neval > 0
+
+
+@pytest.mark.parametrize("family,n,a,u,epsrel", CASES)
+def test_integrate_matches_oracle(cub, oracle, ctx, family, n, a, u, epsrel):
+    f_c = oracle.make_integrand(family, n, a, u)
+    r_c = oracle.Rule(n).integrate_reference(f_c, epsrel, 1e-12)
+    r_g = ctx.integrate(cub.Integrand(family, n, a, u), epsrel, 1e-12)
+    _compare_full(r_g, r_c, oracle.exact(f_c), epsrel, (family, n))
+    # the GPUcuhre mirror gives the same answer
+    q = cub.GPUcuhre(n).integrate(cub.Integrand(family, n, a, u), epsrel, 1e-12)
+    assert q.integral == r_g.integral and q.nregions == r_g.nregions
+
+
+def test_integrate_phase2_matches_oracle(cub, oracle, ctx):
+    """A small phase-1 cap sends leftover boxes through the depth-first
+    second phase on both sides."""
+    n, a, u, eps = 4, [8.0, 12.0, 6.0, 10.0], [0.3, 0.6, 0.5, 0.4], 1e-6
+    f_c = oracle.make_integrand("product_peak", n, a, u)
+    r_c = oracle.Rule(n).integrate_reference(f_c, eps, 1e-12, phase1_cap=512)
+    assert r_c["phase2_regions"] > 0
+    r_g = ctx.integrate(cub.Integrand("product_peak", n, a, u), eps, 1e-12,
+                        cub.options(phase1_cap=512))
+    _compare_full(r_g, r_c, oracle.exact(f_c), eps, "phase2", count_tol=0.05)
+
+
+def test_phase2_failed_boxes_counted(cub, oracle, ctx):
+    """Boxes that hit the bisection cap are counted in the status, as the
+    reference's errorFlag counts failed phase-2 blocks (GPUKernelquad.cu:891)."""
+    n, eps = 3, 1e-9
+    a, u = [40.0, 40.0, 40.0], [0.37, 0.52, 0.61]
+    f_c = oracle.make_integrand("product_peak", n, a, u)
+    r_c = oracle.Rule(n).integrate_reference(f_c, eps, 1e-14, phase1_cap=64, phase2_max=64)
+    r_g = ctx.integrate(cub.Integrand("product_peak", n, a, u), eps, 1e-14,
+                        cub.options(phase1_cap=64, phase2_max_regions=64))
+    assert r_c["status"] > 0
+    assert abs(r_g.status - r_c["status"]) <= max(2, 0.05 * r_c["status"])
+    assert abs(r_g.integral - r_c["value"]) <= 1e-6 * abs(r_c["value"])
+
+
+def test_batch_matches_single(cub, oracle, ctx):
+    rng = np.random.default_rng(3)
+    n, eps = 6, 1e-4
+    params, singles = [], []
+    for k in range(6):
+        a = np.exp(rng.uniform(0, np.log(20), n))
+        u = rng.uniform(0.1, 0.9, n)
+        params.append(cub.make_params(n, list(a), list(u)))
+        singles.append(ctx.integrate(cub.Integrand("product_peak", n, list(a), list(u)), eps,
+                                     1e-12))
+    batch = ctx.integrate_batch("product_peak", n, params, eps, 1e-12)
+    for b, s in zip(batch, singles):
+        assert b.integral == s.integral
+        assert b.error == s.error
+        assert b.nregions == s.nregions and b.status == s.status
+
+
+def test_batch_matches_oracle(cub, oracle, ctx):
+    rng = np.random.default_rng(5)
+    n, eps = 6, 1e-4
+    params, refs = [], []
+    for k in range(5):
+        a = np.exp(rng.uniform(0, np.log(50), n))
+        u = rng.uniform(0.1, 0.9, n)
+        params.append(cub.make_params(n, list(a), list(u)))
+        f_c = oracle.make_integrand("product_peak", n, a, u)
+        refs.append((oracle.Rule(n).integrate_reference(f_c, eps, 1e-12), oracle.exact(f_c)))
+    out = ctx.integrate_batch("product_peak", n, params, eps, 1e-12)
+    for r_g, (r_c, ex) in zip(out, refs):
+        _compare_full(r_g, r_c, ex, eps, "batch")
+
+
+def test_breadth_policy_converges(cub, oracle, ctx):
+    f = cub.Integrand("product_peak", 5, [20.0, 30.0, 10.0, 25.0, 15.0],
+                      [0.3, 0.5, 0.7, 0.45, 0.6])
+    r = ctx.integrate(f, 1e-6, 1e-12, cub.options(policy=cub.POLICY_BREADTH))
+    ex = oracle.exact(oracle.make_integrand("product_peak", 5, f.a, f.u))
+    assert r.status == 0
+    assert abs(r.integral - ex) <= 2e-6 * ex
+
+
+def test_repeatable(cub, ctx):
+    """Fixed-order reductions: two runs give bit-identical results."""
+    f = cub.Integrand("corner_peak", 8, 0.5, 0.0)
+    r1 = ctx.integrate(f, 1e-6, 1e-12)
+    r2 = ctx.integrate(f, 1e-6, 1e-12)
+    assert r1 == r2
