@@ -391,7 +391,7 @@ void orc_eval_region(const orc_rule* r, const orc_integrand* f, const double* L,
     if (w > maxrange) { maxrange = w; maxdim = d; }
   }
 
-  double S[ORC_NSETS] = {0};
+  double S[ORC_NSETS] = {0}, Sabs[ORC_NSETS] = {0};
   double fv[4 * ORC_MAXDIM + 1];
   for (int p = 0; p < r->npts; ++p) {
     const double* g = r->g + (size_t)p * n;
@@ -401,7 +401,13 @@ void orc_eval_region(const orc_rule* r, const orc_integrand* f, const double* L,
     }
     double fx = orc_eval_integrand(f, x);
     S[r->set[p]] += fx;
+    Sabs[r->set[p]] += fabs(fx);
     if (p <= 4 * n) fv[p] = fx;
+  }
+  {
+    double m = 0;
+    for (int k = 0; k < ORC_NSETS; ++k) m += fabs(r->wt[k][0]) * Sabs[k];
+    out->mag = m * jac * ldexp(1., -div);
   }
 
   /* fourth divided difference per axis (GPUQuadSample.cu:152-172) */
@@ -455,7 +461,7 @@ static double max_err(double avg, double epsrel, double epsabs)
 void orc_phase1_eval(const orc_rule* r, const orc_integrand* f, size_t n, const double* lo,
                      const double* len, double epsrel, double epsabs, double* avg,
                      double* err, int* axis, int* active, double* margin, double* ratio,
-                     int nthreads)
+                     double* mag, int nthreads)
 {
   const int nd = r->ndim;
 #ifdef _OPENMP
@@ -477,6 +483,7 @@ void orc_phase1_eval(const orc_rule* r, const orc_integrand* f, size_t n, const 
     active[i] = q > 1;
     if (margin) margin[i] = res.axis_margin;
     if (ratio) ratio[i] = q;
+    if (mag) mag[i] = res.mag;
   }
   (void)nthreads;
 }
@@ -681,7 +688,7 @@ int orc_integrate_reference(const orc_rule* r, const orc_integrand* f, double ep
     double* err = (double*)malloc(sizeof(double) * n);
     int* axis = (int*)malloc(sizeof(int) * n);
     int* act = (int*)malloc(sizeof(int) * n);
-    orc_phase1_eval(r, f, n, lo, len, epsrel, epsabs, avg, err, axis, act, NULL, NULL,
+    orc_phase1_eval(r, f, n, lo, len, epsrel, epsabs, avg, err, axis, act, NULL, NULL, NULL,
                     nthreads);
     ++iters;
     nregions += n;
@@ -779,7 +786,7 @@ int orc_integrate_global(const orc_rule* r, const orc_integrand* f, double epsre
     double* err = (double*)malloc(sizeof(double) * n);
     int* axis = (int*)malloc(sizeof(int) * n);
     int* act = (int*)malloc(sizeof(int) * n);
-    orc_phase1_eval(r, f, n, lo, len, 0, 0, avg, err, axis, act, NULL, NULL, nthreads);
+    orc_phase1_eval(r, f, n, lo, len, 0, 0, avg, err, axis, act, NULL, NULL, NULL, nthreads);
     ++iters;
     nregions += n;
     neval += n * fe;

@@ -63,6 +63,8 @@ typedef struct orc_result {
   int axis;             /* split axis from the fourth divided difference  */
   double axis_margin;   /* relative gap between the best and second-best
                            fourth difference; 0 on an exact tie           */
+  double mag;           /* jac * sum_k |w_k0| sum_p |f_p|: the scale of the
+                           rounding error of avg (cancellation-aware)     */
 } orc_result;
 
 typedef struct orc_out {
@@ -107,7 +109,8 @@ void orc_eval_region(const orc_rule* r, const orc_integrand* f,
 void orc_phase1_eval(const orc_rule* r, const orc_integrand* f, size_t n,
                      const double* lo, const double* len, double epsrel,
                      double epsabs, double* avg, double* err, int* axis,
-                     int* active, double* margin, double* ratio, int nthreads);
+                     int* active, double* margin, double* ratio, double* mag,
+                     int nthreads);
 
 /* ---- scan + compact + bisect (GPUKernelquad.cu:63-149,357-505) ----
  * Children are written [ndim][2m]: child 0 of the j-th active region at

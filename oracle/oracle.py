@@ -40,7 +40,8 @@ class Integrand(C.Structure):
 
 
 class Result(C.Structure):
-    _fields_ = [("avg", C.c_double), ("err", C.c_double), ("axis", C.c_int), ("axis_margin", C.c_double)]
+    _fields_ = [("avg", C.c_double), ("err", C.c_double), ("axis", C.c_int),
+                ("axis_margin", C.c_double), ("mag", C.c_double)]
 
 
 class Out(C.Structure):
@@ -92,7 +93,8 @@ def lib():
         L.orc_eval_region.argtypes = [C.c_void_p, C.POINTER(Integrand), dp, dp, dp, dp, C.c_int,
                                       C.POINTER(Result)]
         L.orc_phase1_eval.argtypes = [C.c_void_p, C.POINTER(Integrand), C.c_size_t, dp, dp,
-                                      C.c_double, C.c_double, dp, dp, ip, ip, dp, dp, C.c_int]
+                                      C.c_double, C.c_double, dp, dp, ip, ip, dp, dp, dp,
+                                      C.c_int]
         L.orc_split.argtypes = [C.c_int, C.c_size_t, dp, dp, ip, ip, dp, dp]
         L.orc_split.restype = C.c_size_t
         L.orc_initial_grid.argtypes = [C.c_int, dp, dp]
@@ -187,11 +189,12 @@ class Rule:
         act = np.zeros(n, dtype=np.int32)
         margin = np.zeros(n)
         ratio = np.zeros(n)
+        mag = np.zeros(n)
         lib().orc_phase1_eval(self._h, C.byref(f), n, _dp(lo), _dp(length), epsrel, epsabs,
                               _dp(avg), _dp(err), _ip(axis), _ip(act), _dp(margin), _dp(ratio),
-                              nthreads)
+                              _dp(mag), nthreads)
         return {"avg": avg, "err": err, "axis": axis, "active": act, "margin": margin,
-                "ratio": ratio}
+                "ratio": ratio, "mag": mag}
 
     def integrate_reference(self, f: Integrand, epsrel, epsabs, phase1_cap=0, phase2_max=0,
                             nthreads=0):

@@ -51,10 +51,13 @@ def refined_list(oracle, n, rounds, seed, frac=0.5):
 
 
 def compare_regions(o, g, label):
-    avg_c, err_c = o["avg"], o["err"]
+    avg_c, err_c, mag = o["avg"], o["err"], o["mag"]
     avg_g, err_g, ax_g, act_g = [t.cpu().numpy() for t in g]
-    assert np.all(np.abs(avg_g - avg_c) <= 1e-13 * np.abs(avg_c) + 1e-300), label
-    assert np.all(np.abs(err_g - err_c) <= 1e-12 * np.abs(avg_c) + 1e-12 * err_c + 1e-300), label
+    # rounding scale: |avg| plus the L1 magnitude of the rule sum (matters
+    # where the integrand cancels over a region)
+    scale = np.abs(avg_c) + mag
+    assert np.all(np.abs(avg_g - avg_c) <= 1e-13 * scale + 1e-300), label
+    assert np.all(np.abs(err_g - err_c) <= 1e-12 * scale + 1e-12 * err_c + 1e-300), label
     clear_axis = o["margin"] > 1e-9
     assert np.array_equal(ax_g[clear_axis], o["axis"][clear_axis]), label
     clear_ratio = np.abs(o["ratio"] - 1) > 1e-8
@@ -216,8 +219,10 @@ def test_batch_matches_single(cub, oracle, ctx):
                                      1e-12))
     batch = ctx.integrate_batch("product_peak", n, params, eps, 1e-12)
     for b, s in zip(batch, singles):
-        assert b.integral == s.integral
-        assert b.error == s.error
+        # the batched path loads parameters from memory instead of kernel
+        # arguments, which may change FMA contraction in the last bit
+        assert abs(b.integral - s.integral) <= 1e-13 * abs(s.integral)
+        assert abs(b.error - s.error) <= 1e-10 * abs(s.error)
         assert b.nregions == s.nregions and b.status == s.status
 
 
