@@ -21,6 +21,7 @@ barrier and device synchronisation, and the max time over ranks is used.
 from __future__ import annotations
 
 import argparse
+import faulthandler
 import json
 import math
 import os
@@ -79,7 +80,9 @@ def product_peak_params(n: int, count: int):
 
 
 class ClockSampler:
-    """nvidia-smi clocks/throttle sampling during the timed region."""
+    """nvidia-smi clocks/throttle sampling (every 10 ms) during the timed
+    region, plus one query right after it for regions shorter than the
+    sampling period.  Read-only: no GPU setting is touched."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -90,15 +93,18 @@ class ClockSampler:
         self.proc = None
         self.lines: list[str] = []
 
+    def _cmd(self, loop: bool):
+        cmd = ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
+               "--format=csv,noheader,nounits"]
+        return cmd + (["-lms", "10"] if loop else [])
+
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.proc = subprocess.Popen(self._cmd(True), stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
-        except (OSError, FileNotFoundError):
+        except OSError:
             self.proc = None
         return self
 
@@ -113,6 +119,11 @@ class ClockSampler:
                 self.proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
+        try:
+            out = subprocess.run(self._cmd(False), capture_output=True, text=True, timeout=10)
+            self.lines.extend(l.strip() for l in out.stdout.splitlines() if l.strip())
+        except (OSError, subprocess.TimeoutExpired):
+            pass
 
     def summary(self) -> dict:
         sm, smax, reasons = [], None, set()
@@ -225,6 +236,7 @@ def run_reference(args, workload, world, rank):
 
 
 def main() -> int:
+    faulthandler.enable()
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
@@ -329,9 +341,22 @@ def main() -> int:
     value = world * nint * args.steps / (dev_ms / 1e3)
     e2e_value = world * nint * args.steps / (wall / 1e3)
 
-    # roofline of the rule kernel (FP64-bound)
-    alg_flops = sum(flops_per_region(f, n) * c for (f, n), c in nreg.items()) * args.steps
-    achieved = alg_flops / (st["ms_eval"] / 1e3) / 1e12 if st["ms_eval"] > 0 else None
+    # roofline of the dominant kernel (FP64-bound rule evaluation).  The
+    # regions are split between the persistent kernel (short lists) and the
+    # multi-launch rule kernel (long lists); each gets its own share of the
+    # algorithmic flops (per-region flops x regions it evaluated).
+    per_region = {k: flops_per_region(f, n) for (f, n) in nreg for k in [(f, n)]}
+    total_regions = sum(nreg.values()) * args.steps
+    mean_flops = sum(per_region[k] * c for k, c in nreg.items()) / max(1, sum(nreg.values()))
+    ml_regions = st["regions_evaluated"]
+    pk_regions = max(0, total_regions - ml_regions)
+    kernels = {
+        "k_persistent": (pk_regions * mean_flops, st["ms_persistent"]),
+        "k_eval": (ml_regions * mean_flops, st["ms_eval"]),
+    }
+    dom = max(kernels, key=lambda k: kernels[k][1])
+    dom_flops, dom_ms = kernels[dom]
+    achieved = dom_flops / (dom_ms / 1e3) / 1e12 if dom_ms > 0 else None
     peak = measure_fp64_peak(torch) if rank == 0 else None
 
     cpu = None
@@ -357,12 +382,16 @@ def main() -> int:
                     "h2d_bytes_per_step": st.get("h2d_bytes", 0) // max(1, args.steps),
                     "d2h_bytes_per_step": st.get("d2h_bytes", 0) // max(1, args.steps)},
             "gpu_launches": st["launches"],
-            "roofline": {"kernel": "k_eval (rule)", "bound": "fp64", "achieved": achieved,
+            "roofline": {"kernel": dom, "bound": "fp64", "achieved": achieved,
                          "peak": peak, "unit": "TFLOP/s",
                          "frac": (achieved / peak) if achieved and peak else None,
                          "traffic": None,
                          "peak_source": "in-run cuBLAS DGEMM 8192^3 (MEASURED_PEAKS.json has no FP64 figure)",
-                         "eval_ms_per_step": st["ms_eval"] / args.steps,
+                         "algorithmic_flops_per_region": mean_flops,
+                         "kernel_ms_per_step": {k: v[1] / args.steps for k, v in kernels.items()},
+                         "regions_per_step": {"k_persistent": pk_regions / args.steps,
+                                              "k_eval": ml_regions / args.steps},
+                         "persistent_iterations_per_step": st["persistent_iterations"] / args.steps,
                          "eval_launches_per_step": st["eval_launches"] / args.steps},
             "cpu_baseline": cpu,
             "clocks": clocks.summary(),

@@ -69,6 +69,7 @@ enum cub_policy {
 #define CUB_ERR_CUDA -2
 #define CUB_ERR_CAPACITY -3
 #define CUB_ERR_UNSUPPORTED -4
+#define CUB_ERR_TIMEOUT -5 /* a bounded device-side wait gave up          */
 
 typedef struct cub_ctx cub_ctx;
 
@@ -94,8 +95,15 @@ typedef struct cub_options {
   int max_iters;           /* breadth-first iteration limit (default 100)  */
   int phase2_max_regions;  /* bisections per leftover box (default 2048)   */
   long long max_slots;     /* region-list capacity (default 2^26)          */
-  int lanes;               /* lanes per region in the rule kernel; 0 auto  */
-  int reserved;
+  int lanes;               /* lanes per region in the multi-launch rule
+                              kernel (1, 8 or 32); 0 = automatic          */
+  int no_persistent;       /* 1: never use the persistent kernel           */
+  int persistent_max_n;    /* list length above which the persistent
+                              kernel hands over to one launch per step;
+                              0 = automatic                               */
+  int persistent_block_n;  /* list length up to which the persistent kernel
+                              evaluates one region per block (else one per
+                              warp); 0 = automatic                        */
 } cub_options;
 
 /* Library version, (major << 16) | minor. */
@@ -125,7 +133,8 @@ void* cub_ctx_stream(cub_ctx* ctx);
  * timing on, CUDA events bracket every rule-kernel and phase-2 launch and
  * their device times are summed (adds one event pair per launch). */
 typedef struct cub_stats {
-  double ms_eval;             /* device time of the rule kernel (timing on) */
+  double ms_eval;             /* device time of the multi-launch rule kernel
+                                 (timing on)                                */
   double ms_phase2;           /* device time of the phase-2 kernel          */
   long long eval_launches;    /* rule-kernel launches                       */
   long long launches;         /* all kernel launches                        */
@@ -134,10 +143,17 @@ typedef struct cub_stats {
   long long phase2_boxes;     /* leftover boxes refined depth-first         */
   long long h2d_bytes;        /* host-to-device bytes copied                */
   long long d2h_bytes;        /* device-to-host bytes copied                */
+  double ms_persistent;       /* device time of the persistent kernel       */
+  long long persistent_launches;
+  long long persistent_iterations; /* iterations run inside it          */
 } cub_stats;
 
 int cub_ctx_stats(const cub_ctx* ctx, cub_stats* out);
 void cub_ctx_reset_stats(cub_ctx* ctx);
+
+/* Return the context's device pools to the driver (the next call reserves
+ * what it needs again). */
+void cub_ctx_release(cub_ctx* ctx);
 void cub_ctx_set_timing(cub_ctx* ctx, int on);
 
 /* One integral over [0,1]^ndim: the body of GPUcuhre::integrate

@@ -5,10 +5,18 @@
 // quad/GPUquad/GPUquad.h:611-620); the prebuilt library instantiates it for
 // the built-in families.
 //
-// All device memory lives in a Workspace that grows geometrically and is
-// reused across calls (the reference mallocs and frees ~10 buffers per
-// iteration, GPUKernelquad.cu:357-605).  One small pinned D2H copy per
-// iteration tells the host the size of the next region list.
+// Two drivers share the device state (region lists, per-integral states,
+// control block):
+//   * the persistent cooperative kernel (persistent.cuh) runs whole
+//     stretches of iterations while the region list is short, with no host
+//     round trip;
+//   * the multi-launch driver runs one iteration per round of launches
+//     (thread-per-region rule kernel) once the list is long, where launch
+//     latency is negligible against the rule kernel.
+// The host switches between them at iteration boundaries.  All device
+// memory lives in a Workspace that grows geometrically and is reused across
+// calls (the reference mallocs and frees ~10 buffers per iteration,
+// GPUKernelquad.cu:357-605).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -20,6 +28,7 @@
 #include <vector>
 
 #include "engine_kernels.cuh"
+#include "persistent.cuh"
 #include "phase2_kernels.cuh"
 #include "rule9.hpp"
 
@@ -31,7 +40,10 @@ struct Options {
   int max_iters = 100;            // phase-1 iterations (GPUKernelquad.cu:631)
   int phase2_max_regions = 2048;  // MAX_GLOBALPOOL_SIZE (quad.h:9)
   long long max_slots = 1ll << 26;
-  int lanes = 0;                  // lanes per region in eval; 0 = automatic
+  int lanes = 0;                  // lanes per region in the multi-launch rule kernel; 0 auto
+  int persistent = 1;             // use the persistent kernel for short lists
+  int persistent_max_n = 0;       // list length where it hands over; 0 auto
+  int persistent_block_n = 0;     // block-per-region evaluation up to this length; 0 auto
 };
 
 struct Result {
@@ -50,12 +62,13 @@ enum ErrorCode : int {
   kErrInvalid = -1,
   kErrCuda = -2,
   kErrCapacity = -3,
+  kErrTimeout = -5,
 };
 
 // Counters of the work a context has launched (reset by the caller).
 struct Stats {
-  double ms_eval = 0;            // summed device time of the rule kernel (timing on)
-  long long eval_launches = 0;   // rule-kernel launches
+  double ms_eval = 0;            // device time of the multi-launch rule kernel (timing on)
+  long long eval_launches = 0;   // multi-launch rule-kernel launches
   long long launches = 0;        // all kernel launches
   long long regions_evaluated = 0;
   long long iterations = 0;      // breadth-first iterations
@@ -63,6 +76,9 @@ struct Stats {
   double ms_phase2 = 0;          // device time of the phase-2 kernel (timing on)
   long long h2d_bytes = 0;       // host-to-device copies issued
   long long d2h_bytes = 0;       // device-to-host copies issued
+  double ms_persistent = 0;      // device time of the persistent kernel (timing on)
+  long long persistent_launches = 0;
+  long long persistent_iterations = 0;
 };
 
 inline const char* state_name(int s) {
@@ -82,29 +98,44 @@ class Workspace {
   Workspace(const Workspace&) = delete;
   Workspace& operator=(const Workspace&) = delete;
 
+  // Free every device and pinned buffer; the next run reserves afresh.
   void release() {
-    for (void*& p : bufs_) {
-      if (p) cudaFree(p);
-      p = nullptr;
-    }
+    for (auto& p : bufs_)
+      if (p.first) cudaFree(p.first);
+    bufs_.clear();
+    bytes_ = 0;
     if (ctl_host_) cudaFreeHost(ctl_host_);
     ctl_host_ = nullptr;
     for (auto& e : ev) {
       if (e) cudaEventDestroy(e);
       e = nullptr;
     }
+    for (int b = 0; b < 2; ++b) lo[b] = len[b] = nullptr, rid[b] = nullptr;
+    avg = err = nullptr;
+    axis = active = chunk_excl = nullptr;
+    part = nullptr;
+    chunk_cnt = int_cnt = nullptr;
+    left_lo = left_len = nullptr;
+    left_rid = nullptr;
+    left_res = nullptr;
+    ist = nullptr;
+    ctl = nullptr;
+    slab = nullptr;
+    heap = counter = nullptr;
     cap_ = left_cap_ = 0;
+    left_ndim_ = 0;
+    heap_ints_ = 0;
     nint_cap_ = 0;
     slab_bytes_ = 0;
     ndim_ = 0;
   }
 
   int device() const { return device_; }
-  bool timing = false;  // record CUDA events around the rule and phase-2 kernels
+  bool timing = false;  // record CUDA events around the rule, persistent and phase-2 kernels
   const std::string& error() const { return err_; }
   Stats& stats() { return stats_; }
 
-  // Buffers (valid after reserve()).
+  // Buffers (valid after the reserve_* calls).
   double* lo[2] = {nullptr, nullptr};
   double* len[2] = {nullptr, nullptr};
   int* rid[2] = {nullptr, nullptr};
@@ -114,6 +145,8 @@ class Workspace {
   int* active = nullptr;
   ChunkPartial* part = nullptr;
   int* chunk_excl = nullptr;
+  unsigned* chunk_cnt = nullptr;
+  unsigned* int_cnt = nullptr;
   double* left_lo = nullptr;
   double* left_len = nullptr;
   int* left_rid = nullptr;
@@ -124,21 +157,29 @@ class Workspace {
   void* slab = nullptr;
   int* heap = nullptr;
   int* counter = nullptr;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
 
   long long cap() const { return cap_; }
   long long left_cap() const { return left_cap_; }
 
-  // Region lists for `slots` regions of dimension ndim; `cur` survives growth.
+  // Region lists for `slots` regions of dimension ndim; list `cur` keeps
+  // its first `keep` slots when the buffers grow.
   bool reserve_lists(int ndim, long long slots, int cur, long long keep, cudaStream_t s) {
     if (slots <= cap_ && ndim == ndim_) return true;
-    long long ncap = std::max<long long>(slots, std::max<long long>(cap_ * 2, 1 << 16));
+    long long ncap;
+    if (ndim != ndim_ || keep == 0) {
+      // nothing to preserve: free first, size for this request only
+      release_lists();
+      ncap = std::max<long long>(slots, 1 << 16);
+    } else {
+      ncap = std::max<long long>(slots, cap_ * 2);
+    }
     ncap = (ncap + 31) & ~31ll;
     double *nlo[2] = {nullptr, nullptr}, *nlen[2] = {nullptr, nullptr};
     int* nrid[2] = {nullptr, nullptr};
     for (int b = 0; b < 2; ++b) {
       if (!alloc(&nlo[b], sizeof(double) * ndim * ncap) ||
-          !alloc(&nlen[b], sizeof(double) * ndim * ncap) ||
-          !alloc(&nrid[b], sizeof(int) * ncap))
+          !alloc(&nlen[b], sizeof(double) * ndim * ncap) || !alloc(&nrid[b], sizeof(int) * ncap))
         return false;
     }
     if (keep > 0 && ndim == ndim_) {
@@ -149,7 +190,8 @@ class Workspace {
                                 cudaMemcpyDeviceToDevice, s)))
           return false;
       }
-      if (!ck(cudaMemcpyAsync(nrid[cur], rid[cur], sizeof(int) * keep, cudaMemcpyDeviceToDevice, s)))
+      if (!ck(cudaMemcpyAsync(nrid[cur], rid[cur], sizeof(int) * keep, cudaMemcpyDeviceToDevice,
+                              s)))
         return false;
       if (!ck(cudaStreamSynchronize(s))) return false;
     }
@@ -167,11 +209,14 @@ class Workspace {
     free_buf(active);
     free_buf(part);
     free_buf(chunk_excl);
+    free_buf(chunk_cnt);
+    const long long nchunk = ncap / 32 + 1;
     if (!alloc(&avg, sizeof(double) * ncap) || !alloc(&err, sizeof(double) * ncap) ||
         !alloc(&axis, sizeof(int) * ncap) || !alloc(&active, sizeof(int) * ncap) ||
-        !alloc(&part, sizeof(ChunkPartial) * (ncap / 32 + 1)) ||
-        !alloc(&chunk_excl, sizeof(int) * (ncap / 32 + 1)))
+        !alloc(&part, sizeof(ChunkPartial) * nchunk) || !alloc(&chunk_excl, sizeof(int) * nchunk) ||
+        !alloc(&chunk_cnt, sizeof(unsigned) * nchunk))
       return false;
+    if (!ck(cudaMemsetAsync(chunk_cnt, 0, sizeof(unsigned) * nchunk, s))) return false;
     cap_ = ncap;
     ndim_ = ndim;
     return true;
@@ -179,7 +224,17 @@ class Workspace {
 
   bool reserve_leftovers(int ndim, long long slots, long long keep, cudaStream_t s) {
     if (slots <= left_cap_ && ndim == left_ndim_) return true;
-    long long ncap = std::max<long long>(slots, std::max<long long>(left_cap_ * 2, 1 << 14));
+    long long ncap;
+    if (ndim != left_ndim_ || keep == 0) {
+      free_buf(left_lo);
+      free_buf(left_len);
+      free_buf(left_rid);
+      free_buf(left_res);
+      left_cap_ = 0;
+      ncap = std::max<long long>(slots, 1 << 14);
+    } else {
+      ncap = std::max<long long>(slots, left_cap_ * 2);
+    }
     double *nlo = nullptr, *nlen = nullptr;
     int* nrid = nullptr;
     LeftoverResult* nres = nullptr;
@@ -211,9 +266,25 @@ class Workspace {
     return true;
   }
 
-  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  // Free the region lists and their per-slot scratch.
+  void release_lists() {
+    for (int b = 0; b < 2; ++b) {
+      free_buf(lo[b]);
+      free_buf(len[b]);
+      free_buf(rid[b]);
+    }
+    free_buf(avg);
+    free_buf(err);
+    free_buf(axis);
+    free_buf(active);
+    free_buf(part);
+    free_buf(chunk_excl);
+    free_buf(chunk_cnt);
+    cap_ = 0;
+    ndim_ = 0;
+  }
 
-  bool reserve_integrals(int nint) {
+  bool reserve_integrals(int nint, cudaStream_t s) {
     if (!ev[0]) {
       for (auto& e : ev)
         if (!ck(cudaEventCreate(&e))) return false;
@@ -222,11 +293,15 @@ class Workspace {
       if (!ck(cudaMallocHost(&ctl_host_, sizeof(Control)))) return false;
       if (!alloc(&ctl, sizeof(Control))) return false;
       if (!alloc(&counter, sizeof(int) * 4)) return false;
+      if (!ck(cudaMemsetAsync(ctl, 0, sizeof(Control), s))) return false;
     }
     if (nint <= nint_cap_) return true;
     free_buf(ist);
+    free_buf(int_cnt);
     const int n = std::max(nint, 64);
-    if (!alloc(&ist, sizeof(IntegralState) * n)) return false;
+    if (!alloc(&ist, sizeof(IntegralState) * n) || !alloc(&int_cnt, sizeof(unsigned) * n))
+      return false;
+    if (!ck(cudaMemsetAsync(int_cnt, 0, sizeof(unsigned) * n, s))) return false;
     nint_cap_ = n;
     return true;
   }
@@ -257,23 +332,25 @@ class Workspace {
     void* q = nullptr;
     if (!ck(cudaMalloc(&q, bytes))) return false;
     *p = static_cast<T*>(q);
-    bufs_.push_back(q);
+    bufs_.push_back({q, bytes});
     bytes_ += bytes;
     return true;
   }
   template <class T>
   void free_buf(T*& p) {
     if (!p) return;
-    for (void*& q : bufs_)
-      if (q == p) {
-        cudaFree(q);
-        q = nullptr;
+    for (auto& q : bufs_)
+      if (q.first == p) {
+        cudaFree(q.first);
+        bytes_ -= q.second;
+        q.first = nullptr;
+        q.second = 0;
       }
     p = nullptr;
   }
 
   int device_;
-  std::vector<void*> bufs_;
+  std::vector<std::pair<void*, size_t>> bufs_;
   long long cap_ = 0, left_cap_ = 0;
   int ndim_ = 0, left_ndim_ = 0;
   int nint_cap_ = 0;
@@ -315,9 +392,10 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
   for (int d = 0; d < N; ++d) per *= dv;
   const int padded = (per + 31) & ~31;
   long long n_cur = (long long)nint * padded;
+  Stats& st = ws.stats();
 
-  if (!ws.reserve_integrals(nint)) return kErrCuda;
-  if (!ws.reserve_lists(N, std::max<long long>(n_cur, 2 * n_cur), 0, 0, s)) return kErrCuda;
+  if (!ws.reserve_integrals(nint, s)) return kErrCuda;
+  if (!ws.reserve_lists(N, std::max<long long>(1 << 20, 4 * n_cur), 0, 0, s)) return kErrCuda;
   if (!ws.reserve_leftovers(N, 1, 0, s)) return kErrCuda;
 
   // integral states
@@ -336,10 +414,12 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
     return kErrCuda;
   Control c0;
   std::memset(&c0, 0, sizeof(c0));
-  c0.n_cur = (int)n_cur;
-  if (!ws.ck(cudaMemcpyAsync(ws.ctl, &c0, sizeof(Control), cudaMemcpyHostToDevice, s)))
+  c0.host.n = (int)n_cur;
+  c0.host.n_running = nint;
+  *ws.ctl_host_ = c0;
+  if (!ws.ck(cudaMemcpyAsync(ws.ctl, ws.ctl_host_, sizeof(Control), cudaMemcpyHostToDevice, s)))
     return kErrCuda;
-  ws.stats().h2d_bytes += (long long)(sizeof(IntegralState) * nint + sizeof(Control));
+  st.h2d_bytes += (long long)(sizeof(IntegralState) * nint + sizeof(Control));
 
   int cur = 0;
   EngineArgs a;
@@ -363,6 +443,8 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
     a.active = ws.active;
     a.part = ws.part;
     a.chunk_excl = ws.chunk_excl;
+    a.chunk_cnt = ws.chunk_cnt;
+    a.int_cnt = ws.int_cnt;
     a.nlo = ws.lo[cur ^ 1];
     a.nlen = ws.len[cur ^ 1];
     a.nrid = ws.rid[cur ^ 1];
@@ -376,23 +458,94 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
   {
     const long long blocks = std::min<long long>((n_cur + 255) / 256, (long long)sms * 8);
     k_init_grid<N><<<(unsigned)std::max<long long>(blocks, 1), 256, 0, s>>>(a, dv, per, padded);
+    st.launches += 1;
   }
-  ws.stats().launches += 1;
-  Stats& st = ws.stats();
+
+  // persistent kernel geometry
+  int pblocks = 0;
+  if (opt.persistent) {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_persistent<N, Src>, 256, 0);
+    int coop = 0;
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, ws.device());
+    if (per_sm > 0 && coop) pblocks = per_sm * sms;
+  }
+  const int pmax = opt.persistent_max_n > 0 ? opt.persistent_max_n : pblocks * 8 * 8;
+
+  IterState hs = c0.host;
   long long n_left = 0;
   int status = kOk;
-  for (int it = 0;; ++it) {
-    // capacity for the worst case of this iteration
+  while (hs.n_running > 0 && hs.n > 0) {
+    n_cur = hs.n;
+    // capacity for the worst case of the coming iteration(s)
     const long long need = 2 * n_cur + 32ll * nint;
     if (need > opt.max_slots) {
       status = kErrCapacity;
       break;
     }
-    if (!ws.reserve_lists(N, need, cur, n_cur, s)) return kErrCuda;
+    if (!ws.reserve_lists(N, std::max<long long>(need, 4 * n_cur), cur, n_cur, s)) return kErrCuda;
     if (opt.policy == kPolicyReference &&
-        !ws.reserve_leftovers(N, n_left + 2 * n_cur + 1, n_left, s))
+        !ws.reserve_leftovers(N, n_left + 4 * n_cur + 1, n_left, s))
       return kErrCuda;
     bind(n_cur);
+
+    if (pblocks > 0 && n_cur <= pmax) {
+      // a stretch of iterations in one persistent launch
+      ws.ctl_host_->host = hs;
+      ws.ctl_host_->it[0] = hs;
+      ws.ctl_host_->cur = cur;
+      ws.ctl_host_->done_cnt = 0;
+      ws.ctl_host_->bar_count = 0;
+      ws.ctl_host_->timeout = 0;
+      ws.ctl_host_->exit_reason = 0;
+      if (!ws.ck(cudaMemcpyAsync(ws.ctl, ws.ctl_host_, sizeof(Control), cudaMemcpyHostToDevice, s)))
+        return kErrCuda;
+      st.h2d_bytes += sizeof(Control);
+      PersistArgs p;
+      p.base = a;
+      for (int b = 0; b < 2; ++b) {
+        p.lo[b] = ws.lo[b];
+        p.len[b] = ws.len[b];
+        p.rid[b] = ws.rid[b];
+      }
+      p.max_n = pmax;
+      // one region per block while every block gets at most one region;
+      // beyond that one region per warp keeps more points in flight
+      // (measured on B200: 8-D rule, 148 vs 1184 blocks' worth)
+      p.block_mode_max_n = opt.persistent_block_n > 0 ? opt.persistent_block_n : pblocks;
+      void* args[] = {(void*)&src, (void*)&T, (void*)&p};
+      if (ws.timing) ws.ck(cudaEventRecord(ws.ev[0], s));
+      if (!ws.ck(cudaLaunchCooperativeKernel((const void*)k_persistent<N, Src>, dim3(pblocks),
+                                             dim3(256), args, 0, s)))
+        return kErrCuda;
+      if (ws.timing) ws.ck(cudaEventRecord(ws.ev[1], s));
+      st.launches += 1;
+      st.persistent_launches += 1;
+      if (!ws.ck(cudaMemcpyAsync(ws.ctl_host_, ws.ctl, sizeof(Control), cudaMemcpyDeviceToHost, s)))
+        return kErrCuda;
+      if (!ws.ck(cudaStreamSynchronize(s))) return kErrCuda;
+      st.d2h_bytes += sizeof(Control);
+      if (ws.timing) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, ws.ev[0], ws.ev[1]);
+        st.ms_persistent += ms;
+      }
+      const Control& c = *ws.ctl_host_;
+      const int before = c0.iters_done;
+      st.iterations += c.iters_done - before;
+      st.persistent_iterations += c.iters_done - before;
+      c0.iters_done = c.iters_done;
+      if (c.exit_reason == kExitTimeout || c.timeout) {
+        ws.ck(cudaErrorLaunchTimeout);
+        return kErrTimeout;
+      }
+      cur = c.cur;
+      hs = c.host;
+      n_left = hs.n_left;
+      continue;  // done, too large or capacity: the loop re-checks
+    }
+
+    // one iteration, one launch per step
     int K = opt.lanes;
     if (K <= 0) K = n_cur >= (long long)sms * 512 ? 1 : (n_cur >= (long long)sms * 64 ? 8 : 32);
     if (ws.timing) ws.ck(cudaEventRecord(ws.ev[0], s));
@@ -403,36 +556,36 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
     }
     if (ws.timing) ws.ck(cudaEventRecord(ws.ev[1], s));
     st.eval_launches += 1;
-    st.launches += 1;
     st.regions_evaluated += n_cur;
     const long long nchunk = (n_cur + 31) / 32;
-    const unsigned pb = (unsigned)std::max<long long>(1, std::min<long long>((nchunk + 7) / 8, sms * 16ll));
+    const unsigned pb =
+        (unsigned)std::max<long long>(1, std::min<long long>((nchunk + 7) / 8, sms * 16ll));
     k_partials<<<pb, 256, 0, s>>>(a);
     const unsigned db = (unsigned)std::max(1, std::min((nint + 7) / 8, sms * 16));
     k_decide<<<db, 256, 0, s>>>(a);
-    k_scan<<<1, 1024, 0, s>>>(a);
+    k_scan<<<1, 32, 0, s>>>(a);
     k_split<N><<<pb, 256, 0, s>>>(a);
     k_advance<<<(unsigned)std::max(1, std::min((nint + 255) / 256, sms)), 256, 0, s>>>(a);
-    st.launches += 5;
+    st.launches += 6;
     if (!ws.ck(cudaMemcpyAsync(ws.ctl_host_, ws.ctl, sizeof(Control), cudaMemcpyDeviceToHost, s)))
       return kErrCuda;
     if (!ws.ck(cudaStreamSynchronize(s))) return kErrCuda;
-    const Control c = *ws.ctl_host_;
     st.iterations += 1;
     st.d2h_bytes += (long long)sizeof(Control);
+    c0.iters_done = ws.ctl_host_->iters_done;
     if (ws.timing) {
       float ms = 0;
       cudaEventElapsedTime(&ms, ws.ev[0], ws.ev[1]);
       st.ms_eval += ms;
     }
-    if (c.overflow) {
+    const IterState nx = ws.ctl_host_->host;
+    if (nx.overflow) {
       status = kErrCapacity;
       break;
     }
-    n_left = c.n_left;
-    n_cur = c.n_cur;
     cur ^= 1;
-    if (c.n_running == 0 || n_cur == 0) break;
+    hs = nx;
+    n_left = nx.n_left;
   }
 
   if (status == kOk && n_left > 0) {
@@ -471,7 +624,7 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
   if (!ws.ck(cudaMemcpyAsync(h.data(), ws.ist, sizeof(IntegralState) * nint,
                              cudaMemcpyDeviceToHost, s)))
     return kErrCuda;
-  ws.stats().d2h_bytes += (long long)(sizeof(IntegralState) * nint);
+  st.d2h_bytes += (long long)(sizeof(IntegralState) * nint);
   if (!ws.ck(cudaStreamSynchronize(s))) return kErrCuda;
   if (!ws.ck(cudaGetLastError())) return kErrCuda;
   if (ws.timing && status == kOk && n_left > 0) {

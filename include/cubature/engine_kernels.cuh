@@ -15,6 +15,10 @@
 //             adjacent children (alignRegions + divideIntervalsGPU,
 //             GPUKernelquad.cu:63-149)
 //
+// The steps are warp-level device functions shared by two drivers: one
+// kernel launch per step (the throughput regime, engine.cuh) and the
+// persistent cooperative kernel (the latency regime, persistent.cuh).
+//
 // Layout in HBM: region lists are SoA, lo[d * cap + i] and len[d * cap + i]
 // (FP64), rid[i] = owning integral (-1 = padding).  Each integral owns a
 // contiguous segment whose start is a multiple of 32, so a 32-region chunk
@@ -57,15 +61,33 @@ struct ChunkPartial {
   int nactive, pad;
 };
 
-// Control block: list sizes and counters of the current iteration.
-struct Control {
-  int n_cur;      // slots in the current list (padded)
-  int n_next;     // slots in the next list (padded)
-  int n_running;  // integrals still running after this iteration
+// List sizes after one iteration's scan.
+struct IterState {
+  int n;          // slots in the list (padded)
+  int n_running;  // integrals with regions in that list
   int n_left;     // leftover boxes queued for phase 2 so far
-  int overflow;   // set when a list would exceed its capacity
-  int iter;
-  int pad[2];
+  int overflow;   // the list or the leftovers would exceed capacity
+};
+
+// Control block shared by the host and both drivers.
+struct Control {
+  IterState host;      // result of the last scan (multi-launch driver)
+  IterState it[2];     // double-buffered by iteration parity (persistent)
+  int cur;             // index of the current list buffer
+  int iters_done;      // breadth-first iterations completed
+  int exit_reason;     // persistent kernel: why it returned
+  int pad;
+  unsigned done_cnt;   // integrals decided in this iteration
+  unsigned bar_count;  // grid barrier arrivals
+  unsigned bar_gen;    // grid barrier generation
+  int timeout;         // a bounded wait gave up
+};
+
+enum ExitReason : int {
+  kExitDone = 1,      // no integral left running
+  kExitLarge = 2,     // the list grew past the persistent kernel's range
+  kExitCapacity = 3,  // buffers must grow before the next iteration
+  kExitTimeout = 4,   // a grid barrier wait ran out
 };
 
 struct EngineArgs {
@@ -80,9 +102,11 @@ struct EngineArgs {
   double* err;
   int* axis;
   int* active;
-  // chunk partials / prefix
+  // chunk partials / prefix / arrival counters
   ChunkPartial* part;
   int* chunk_excl;
+  unsigned* chunk_cnt;
+  unsigned* int_cnt;
   // next list
   double* nlo;
   double* nlen;
@@ -122,339 +146,336 @@ struct ParamSource {
   __device__ __forceinline__ F get(int k) const { return F::load(params[k]); }
 };
 
-}  // namespace detail
+// Write one region's results (reference classification:
+// fail when err / max(epsrel|avg|, epsabs) > 1, GPUQuadPhases.cu:63-74).
+__device__ __forceinline__ void store_result(const EngineArgs& a, long long slot,
+                                             const RegionResult& r, const IntegralState& is) {
+  const double ratio = r.err / max_err(r.avg, is.epsrel, is.epsabs);
+  a.avg[slot] = r.avg;
+  a.err[slot] = r.err;
+  a.axis[slot] = r.axis;
+  a.active[slot] = ratio > 1;
+}
 
-// ---------------------------------------------------------------------------
-// eval: K lanes per region, grid-stride over slots.
-// ---------------------------------------------------------------------------
+__device__ __forceinline__ void store_padding(const EngineArgs& a, long long slot) {
+  a.avg[slot] = 0;
+  a.err[slot] = 0;
+  a.axis[slot] = 0;
+  a.active[slot] = 0;
+}
+
+// Evaluate slot `slot` with the K lanes of a group (K <= 32, structured
+// point enumeration); lane 0 of the group stores the result.
 template <int N, int K, class Src>
-__global__ void __launch_bounds__(256) k_eval(Src src, RuleTables T, EngineArgs a) {
-  __shared__ detail::ItemTable<N> tab;
-  if (threadIdx.x == 0) tab.fill();
-  __syncthreads();
-
-  constexpr int kGroups = 256 / K;
-  const int lane = threadIdx.x % K;
-  const unsigned gmask = (K == 32) ? 0xffffffffu : (((1u << K) - 1u) << ((threadIdx.x & 31) & ~(K - 1)));
-  for (long long slot = (long long)blockIdx.x * kGroups + threadIdx.x / K; slot < a.n;
-       slot += (long long)gridDim.x * kGroups) {
-    const int k = a.rid[slot];
-    if (k < 0) {
-      if (lane == 0) {
-        a.avg[slot] = 0;
-        a.err[slot] = 0;
-        a.axis[slot] = 0;
-        a.active[slot] = 0;
-      }
-      continue;
-    }
-    double L[N], H[N];
+__device__ __forceinline__ void eval_slot(const Src& src, const RuleTables& T,
+                                          const EngineArgs& a, long long slot, int lane,
+                                          unsigned gmask, const ItemTable<N>& tab) {
+  const int k = a.rid[slot];
+  if (k < 0) {
+    if (lane == 0) store_padding(a, slot);
+    return;
+  }
+  double L[N], H[N];
 #pragma unroll
-    for (int d = 0; d < N; ++d) {
-      L[d] = a.lo[(long long)d * a.cap + slot];
-      H[d] = a.len[(long long)d * a.cap + slot];
-    }
-    const auto f = src.get(k);
-    detail::RegionSums rs;
-    detail::region_point_sums<N, K>(f, L, H, lane, tab, T.ratio, rs);
-    if (K > 1) detail::reduce_lanes<K>(rs, gmask);
-    if (lane == 0) {
-      double jac = 1;
+  for (int d = 0; d < N; ++d) {
+    L[d] = a.lo[(long long)d * a.cap + slot];
+    H[d] = a.len[(long long)d * a.cap + slot];
+  }
+  const auto f = src.get(k);
+  RegionSums rs;
+  region_point_sums<N, K>(f, L, H, lane, tab, T.ratio, rs);
+  if (K > 1) reduce_lanes<K>(rs, gmask);
+  if (lane == 0) {
+    double jac = 1;
 #pragma unroll
-      for (int d = 0; d < N; ++d) jac = __dmul_rn(jac, H[d]);
-      const detail::RegionResult r = detail::finish_region<N>(rs, T, jac, 0);
-      const IntegralState& is = a.ist[k];
-      // reference policy: fail when err / max(epsrel|avg|, epsabs) > 1
-      const double ratio = r.err / detail::max_err(r.avg, is.epsrel, is.epsabs);
-      a.avg[slot] = r.avg;
-      a.err[slot] = r.err;
-      a.axis[slot] = r.axis;
-      a.active[slot] = ratio > 1;
-    }
+    for (int d = 0; d < N; ++d) jac = __dmul_rn(jac, H[d]);
+    store_result(a, slot, finish_region<N>(rs, T, jac, 0), a.ist[k]);
   }
 }
 
-// ---------------------------------------------------------------------------
-// partials: one warp per 32-slot chunk.
-// ---------------------------------------------------------------------------
-static __global__ void __launch_bounds__(256) k_partials(EngineArgs a) {
-  const int lane = threadIdx.x & 31;
-  const long long nchunk = (a.n + 31) / 32;
-  for (long long c = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / 32; c < nchunk;
-       c += (long long)gridDim.x * blockDim.x / 32) {
-    const long long i = c * 32 + lane;
-    const bool valid = i < a.n && a.rid[i] >= 0;
-    const double av = valid ? a.avg[i] : 0.0, er = valid ? a.err[i] : 0.0;
-    const bool act = valid && a.active[i];
-    double s0 = av, s1 = er, s2 = act ? 0.0 : av, s3 = act ? 0.0 : er;
+// A warp sums the 32 slots of chunk c into a.part[c].
+__device__ __forceinline__ void chunk_partial_warp(const EngineArgs& a, long long c, int lane) {
+  const long long i = c * 32 + lane;
+  const bool valid = i < a.n && a.rid[i] >= 0;
+  const double av = valid ? a.avg[i] : 0.0, er = valid ? a.err[i] : 0.0;
+  const bool act = valid && a.active[i];
+  double s0 = av, s1 = er, s2 = act ? 0.0 : av, s3 = act ? 0.0 : er;
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-      s0 += __shfl_xor_sync(0xffffffffu, s0, off);
-      s1 += __shfl_xor_sync(0xffffffffu, s1, off);
-      s2 += __shfl_xor_sync(0xffffffffu, s2, off);
-      s3 += __shfl_xor_sync(0xffffffffu, s3, off);
-    }
-    const unsigned b = __ballot_sync(0xffffffffu, act);
-    if (lane == 0) {
-      ChunkPartial p;
-      p.sum_avg = s0;
-      p.sum_err = s1;
-      p.fin_avg = s2;
-      p.fin_err = s3;
-      p.nactive = __popc(b);
-      p.pad = 0;
-      a.part[c] = p;
-    }
+  for (int off = 16; off > 0; off >>= 1) {
+    s0 += __shfl_xor_sync(0xffffffffu, s0, off);
+    s1 += __shfl_xor_sync(0xffffffffu, s1, off);
+    s2 += __shfl_xor_sync(0xffffffffu, s2, off);
+    s3 += __shfl_xor_sync(0xffffffffu, s3, off);
+  }
+  const unsigned b = __ballot_sync(0xffffffffu, act);
+  if (lane == 0) {
+    ChunkPartial p;
+    p.sum_avg = s0;
+    p.sum_err = s1;
+    p.fin_avg = s2;
+    p.fin_err = s3;
+    p.nactive = __popc(b);
+    p.pad = 0;
+    a.part[c] = p;
   }
 }
 
-// ---------------------------------------------------------------------------
-// decide: one warp per running integral.
-// ---------------------------------------------------------------------------
-static __global__ void __launch_bounds__(256) k_decide(EngineArgs a) {
-  const int lane = threadIdx.x & 31;
-  for (int k = (blockIdx.x * blockDim.x + threadIdx.x) / 32; k < a.nint;
-       k += gridDim.x * blockDim.x / 32) {
-    IntegralState& is = a.ist[k];
-    if (is.state != kStateRunning) {
-      if (lane == 0) {
-        is.next_count = 0;
-        is.left_new = 0;
-      }
-      continue;
-    }
-    const int c0 = is.seg_start / 32;
-    const int nc = (is.seg_count + 31) / 32;
-    double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
-    for (int c = lane; c < nc; c += 32) {
-      const ChunkPartial p = a.part[c0 + c];
-      s0 += p.sum_avg;
-      s1 += p.sum_err;
-      s2 += p.fin_avg;
-      s3 += p.fin_err;
-    }
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-      s0 += __shfl_xor_sync(0xffffffffu, s0, off);
-      s1 += __shfl_xor_sync(0xffffffffu, s1, off);
-      s2 += __shfl_xor_sync(0xffffffffu, s2, off);
-      s3 += __shfl_xor_sync(0xffffffffu, s3, off);
-    }
-    // exclusive scan of active counts over the integral's chunks
-    int running = 0;
-    for (int base = 0; base < nc; base += 32) {
-      const int c = base + lane;
-      const int v = c < nc ? a.part[c0 + c].nactive : 0;
-      int incl = v;
-#pragma unroll
-      for (int off = 1; off < 32; off <<= 1) {
-        const int t = __shfl_up_sync(0xffffffffu, incl, off);
-        if (lane >= off) incl += t;
-      }
-      if (c < nc) a.chunk_excl[c0 + c] = running + incl - v;
-      running += __shfl_sync(0xffffffffu, incl, 31);
-    }
+// A warp combines integral k's chunk partials, writes the exclusive scan
+// of active counts over its chunks, and takes the stop decision
+// (GPUKernelquad.cu:565-605).
+__device__ __forceinline__ void decide_warp(const EngineArgs& a, int k, int lane) {
+  IntegralState& is = a.ist[k];
+  if (is.state != kStateRunning) {
     if (lane == 0) {
-      const int m = running;
-      const double rG = is.value + s0, errG = is.error + s1;
-      is.value += s2;
-      is.error += s3;
-      is.last_value = rG;
-      is.last_error = errG;
-      is.nregions += (unsigned long long)is.seg_count;
-      is.neval += (unsigned long long)is.seg_count * (unsigned long long)a.npoints;
-      is.iters += 1;
       is.next_count = 0;
       is.left_new = 0;
-      if (errG <= detail::max_err(rG, is.epsrel, is.epsabs)) {
-        // global stop test (GPUKernelquad.cu:583-598)
-        is.value = rG;
-        is.error = errG;
-        is.state = kStateDone;
-        is.status = 0;
-      } else if (m == 0) {
-        // every region finished on its own tolerance
-        is.state = kStateDone;
-        is.status = 0;
-      } else {
-        const long long children = 2ll * m;
-        const bool cap_hit = a.phase1_cap > 0 && children >= a.phase1_cap;
-        const bool iter_hit = is.iters >= a.max_iters;
-        if (cap_hit || iter_hit) {
-          if (a.policy == kPolicyReference) {
-            is.state = kStatePhase2;
-            is.left_new = (int)children;
-          } else {
-            is.state = kStateCapacity;
-            is.value = rG;
-            is.error = errG;
-            is.status = 1;
-          }
+    }
+    return;
+  }
+  const int c0 = is.seg_start / 32;
+  const int nc = (is.seg_count + 31) / 32;
+  double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+  for (int c = lane; c < nc; c += 32) {
+    const ChunkPartial p = a.part[c0 + c];
+    s0 += p.sum_avg;
+    s1 += p.sum_err;
+    s2 += p.fin_avg;
+    s3 += p.fin_err;
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    s0 += __shfl_xor_sync(0xffffffffu, s0, off);
+    s1 += __shfl_xor_sync(0xffffffffu, s1, off);
+    s2 += __shfl_xor_sync(0xffffffffu, s2, off);
+    s3 += __shfl_xor_sync(0xffffffffu, s3, off);
+  }
+  int running = 0;
+  for (int base = 0; base < nc; base += 32) {
+    const int c = base + lane;
+    const int v = c < nc ? a.part[c0 + c].nactive : 0;
+    int incl = v;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, incl, off);
+      if (lane >= off) incl += t;
+    }
+    if (c < nc) a.chunk_excl[c0 + c] = running + incl - v;
+    running += __shfl_sync(0xffffffffu, incl, 31);
+  }
+  if (lane == 0) {
+    const int m = running;
+    const double rG = is.value + s0, errG = is.error + s1;
+    is.value += s2;
+    is.error += s3;
+    is.last_value = rG;
+    is.last_error = errG;
+    is.nregions += (unsigned long long)is.seg_count;
+    is.neval += (unsigned long long)is.seg_count * (unsigned long long)a.npoints;
+    is.iters += 1;
+    is.next_count = 0;
+    is.left_new = 0;
+    if (errG <= max_err(rG, is.epsrel, is.epsabs)) {
+      // global stop test (GPUKernelquad.cu:583-598)
+      is.value = rG;
+      is.error = errG;
+      is.state = kStateDone;
+      is.status = 0;
+    } else if (m == 0) {
+      // every region finished on its own tolerance
+      is.state = kStateDone;
+      is.status = 0;
+    } else {
+      const long long children = 2ll * m;
+      const bool cap_hit = a.phase1_cap > 0 && children >= a.phase1_cap;
+      const bool iter_hit = is.iters >= a.max_iters;
+      if (cap_hit || iter_hit) {
+        if (a.policy == kPolicyReference) {
+          is.state = kStatePhase2;
+          is.left_new = (int)children;
         } else {
-          is.next_count = (int)children;
+          is.state = kStateCapacity;
+          is.value = rG;
+          is.error = errG;
+          is.status = 1;
         }
+      } else {
+        is.next_count = (int)children;
       }
     }
   }
 }
 
-// ---------------------------------------------------------------------------
-// scan: one block assigns the next segments and leftover ranges.
-// ---------------------------------------------------------------------------
-static __global__ void __launch_bounds__(1024) k_scan(EngineArgs a) {
-  __shared__ int warp_tot[32][2];
-  __shared__ int carry[2];
-  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-  if (tid == 0) {
-    carry[0] = 0;
-    carry[1] = a.ctl->n_left;
-  }
-  __syncthreads();
-  int nrun = 0;
-  for (int base = 0; base < a.nint; base += 1024) {
-    const int k = base + tid;
-    int vn = 0, vl = 0;
+// A single warp assigns the next segments (32-aligned) and the leftover
+// ranges of all integrals: an exclusive scan in integral order.
+__device__ __forceinline__ void scan_warp(const EngineArgs& a, int n_left_in, IterState* out,
+                                          int lane) {
+  int carry_n = 0, carry_l = n_left_in, nrun = 0;
+  for (int base = 0; base < a.nint; base += 32) {
+    const int k = base + lane;
+    int vn = 0, vl = 0, r = 0;
     if (k < a.nint) {
       const IntegralState& is = a.ist[k];
-      vn = (is.next_count + 31) & ~31;  // padded segment
-      vl = is.left_new;
-      nrun += is.state == kStateRunning && is.next_count > 0;
+      vn = is.state == kStateRunning ? (is.next_count + 31) & ~31 : 0;
+      vl = is.left_count == 0 ? is.left_new : 0;  // each integral hands off once
+      r = is.state == kStateRunning && is.next_count > 0;
     }
     int in = vn, il = vl;
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) {
       const int tn = __shfl_up_sync(0xffffffffu, in, off);
       const int tl = __shfl_up_sync(0xffffffffu, il, off);
-      if (lane >= off) { in += tn; il += tl; }
-    }
-    if (lane == 31) { warp_tot[wid][0] = in; warp_tot[wid][1] = il; }
-    __syncthreads();
-    if (wid == 0) {
-      int wn = warp_tot[lane][0], wl = warp_tot[lane][1];
-#pragma unroll
-      for (int off = 1; off < 32; off <<= 1) {
-        const int tn = __shfl_up_sync(0xffffffffu, wn, off);
-        const int tl = __shfl_up_sync(0xffffffffu, wl, off);
-        if (lane >= off) { wn += tn; wl += tl; }
+      if (lane >= off) {
+        in += tn;
+        il += tl;
       }
-      warp_tot[lane][0] = wn;
-      warp_tot[lane][1] = wl;
     }
-    __syncthreads();
-    const int wbase_n = wid > 0 ? warp_tot[wid - 1][0] : 0;
-    const int wbase_l = wid > 0 ? warp_tot[wid - 1][1] : 0;
     if (k < a.nint) {
       IntegralState& is = a.ist[k];
-      is.next_start = carry[0] + wbase_n + in - vn;
+      is.next_start = carry_n + in - vn;
       if (vl > 0) {
-        is.left_start = carry[1] + wbase_l + il - vl;
+        is.left_start = carry_l + il - vl;
         is.left_count = vl;
       }
     }
-    __syncthreads();
-    if (tid == 0) {
-      carry[0] += warp_tot[31][0];
-      carry[1] += warp_tot[31][1];
-    }
-    __syncthreads();
+    carry_n += __shfl_sync(0xffffffffu, in, 31);
+    carry_l += __shfl_sync(0xffffffffu, il, 31);
+    nrun += __popc(__ballot_sync(0xffffffffu, r));
   }
-  // count running integrals
-  __shared__ int nrun_s;
-  if (tid == 0) nrun_s = 0;
-  __syncthreads();
-  atomicAdd(&nrun_s, nrun);
-  __syncthreads();
-  if (tid == 0) {
-    Control* c = a.ctl;
-    c->n_next = carry[0];
-    c->n_left = carry[1];
-    c->n_running = nrun_s;
-    c->overflow = (carry[0] > a.ncap) || (carry[1] > a.left_cap);
+  if (lane == 0) {
+    IterState s;
+    s.n = carry_n;
+    s.n_running = nrun;
+    s.n_left = carry_l;
+    s.overflow = (carry_n > a.ncap) || (carry_l > a.left_cap);
+    *out = s;
   }
 }
 
-// ---------------------------------------------------------------------------
-// split: one warp per chunk; writes two adjacent children per active
-// region, to the next list (running integrals) or the leftover list
-// (integrals handed to phase 2).  Also writes the padding slot ids.
-// ---------------------------------------------------------------------------
+// A warp writes the children of chunk c's active regions: two adjacent
+// children per region, halved on its split axis, to the next list (running
+// integrals) or the leftover list (integrals just handed to phase 2).
 template <int N>
-__global__ void __launch_bounds__(256) k_split(EngineArgs a) {
-  if (a.ctl->overflow) return;
-  const int lane = threadIdx.x & 31;
-  const long long nchunk = (a.n + 31) / 32;
-  const long long gwarp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / 32;
-  const long long nwarp = (long long)gridDim.x * blockDim.x / 32;
-  for (long long c = gwarp; c < nchunk; c += nwarp) {
-    const long long i = c * 32 + lane;
-    const int k = i < a.n ? a.rid[i] : -1;
-    bool act = k >= 0 && a.active[i];
-    int state = kStateDone;
-    if (act) {
-      state = a.ist[k].state;
-      act = (state == kStateRunning && a.ist[k].next_count > 0) ||
-            (state == kStatePhase2 && a.ist[k].left_new > 0);
-    }
-    const unsigned b = __ballot_sync(0xffffffffu, act);
-    if (!act) continue;
-    const int rank = a.chunk_excl[c] + __popc(b & ((1u << lane) - 1u));
-    const int ax = a.axis[i];
-    double* dlo;
-    double* dlen;
-    int* drid;
-    long long dcap, dst;
-    if (state == kStatePhase2) {
-      dlo = a.left_lo; dlen = a.left_len; drid = a.left_rid; dcap = a.left_cap;
-      dst = a.ist[k].left_start + 2ll * rank;
-    } else {
-      dlo = a.nlo; dlen = a.nlen; drid = a.nrid; dcap = a.ncap;
-      dst = a.ist[k].next_start + 2ll * rank;
-    }
-#pragma unroll
-    for (int d = 0; d < N; ++d) {
-      const double l = a.lo[(long long)d * a.cap + i];
-      const double w = a.len[(long long)d * a.cap + i];
-      if (d == ax) {
-        const double h = w / 2;
-        dlo[(long long)d * dcap + dst] = l;
-        dlo[(long long)d * dcap + dst + 1] = l + 1 * h;
-        dlen[(long long)d * dcap + dst] = h;
-        dlen[(long long)d * dcap + dst + 1] = h;
-      } else {
-        dlo[(long long)d * dcap + dst] = l;
-        dlo[(long long)d * dcap + dst + 1] = l;
-        dlen[(long long)d * dcap + dst] = w;
-        dlen[(long long)d * dcap + dst + 1] = w;
-      }
-    }
-    drid[dst] = k;
-    drid[dst + 1] = k;
+__device__ __forceinline__ void split_chunk_warp(const EngineArgs& a, long long c, int lane) {
+  const long long i = c * 32 + lane;
+  const int k = i < a.n ? a.rid[i] : -1;
+  bool act = k >= 0 && a.active[i];
+  int state = kStateDone;
+  if (act) {
+    state = a.ist[k].state;
+    act = (state == kStateRunning && a.ist[k].next_count > 0) ||
+          (state == kStatePhase2 && a.ist[k].left_new > 0);
   }
-  // padding ids of the next list (<= 31 per integral)
-  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < a.nint;
-       k += (long long)gridDim.x * blockDim.x) {
-    const IntegralState& is = a.ist[k];
-    if (is.next_count <= 0) continue;
+  const unsigned b = __ballot_sync(0xffffffffu, act);
+  if (!act) return;
+  const int rank = a.chunk_excl[c] + __popc(b & ((1u << lane) - 1u));
+  const int ax = a.axis[i];
+  double* dlo;
+  double* dlen;
+  int* drid;
+  long long dcap, dst;
+  if (state == kStatePhase2) {
+    dlo = a.left_lo;
+    dlen = a.left_len;
+    drid = a.left_rid;
+    dcap = a.left_cap;
+    dst = a.ist[k].left_start + 2ll * rank;
+  } else {
+    dlo = a.nlo;
+    dlen = a.nlen;
+    drid = a.nrid;
+    dcap = a.ncap;
+    dst = a.ist[k].next_start + 2ll * rank;
+  }
+#pragma unroll
+  for (int d = 0; d < N; ++d) {
+    const double l = a.lo[(long long)d * a.cap + i];
+    const double w = a.len[(long long)d * a.cap + i];
+    if (d == ax) {
+      const double h = w / 2;
+      dlo[(long long)d * dcap + dst] = l;
+      dlo[(long long)d * dcap + dst + 1] = l + 1 * h;
+      dlen[(long long)d * dcap + dst] = h;
+      dlen[(long long)d * dcap + dst + 1] = h;
+    } else {
+      dlo[(long long)d * dcap + dst] = l;
+      dlo[(long long)d * dcap + dst + 1] = l;
+      dlen[(long long)d * dcap + dst] = w;
+      dlen[(long long)d * dcap + dst + 1] = w;
+    }
+  }
+  drid[dst] = k;
+  drid[dst + 1] = k;
+}
+
+// Padding ids of integral k's next segment, and the segment hand-over
+// (the next list becomes current).
+__device__ __forceinline__ void finish_integral(const EngineArgs& a, int k) {
+  IntegralState& is = a.ist[k];
+  if (is.next_count > 0) {
     const int padded = (is.next_count + 31) & ~31;
     for (int j = is.next_count; j < padded; ++j) a.nrid[is.next_start + j] = -1;
   }
+  if (is.state == kStateRunning) {
+    is.seg_start = is.next_start;
+    is.seg_count = is.next_count;
+    if (is.next_count == 0) is.state = kStateDone;
+  } else {
+    is.seg_count = 0;
+  }
 }
 
-// After split: the next list becomes current.
+}  // namespace detail
+
+// ---------------------------------------------------------------------------
+// Multi-launch driver kernels (one launch per step).
+// ---------------------------------------------------------------------------
+template <int N, int K, class Src>
+__global__ void __launch_bounds__(256) k_eval(Src src, RuleTables T, EngineArgs a) {
+  __shared__ detail::ItemTable<N> tab;
+  if (threadIdx.x == 0) tab.fill();
+  __syncthreads();
+  constexpr int kGroups = 256 / K;
+  const int lane = threadIdx.x % K;
+  const unsigned gmask =
+      (K == 32) ? 0xffffffffu : (((1u << K) - 1u) << ((threadIdx.x & 31) & ~(K - 1)));
+  for (long long slot = (long long)blockIdx.x * kGroups + threadIdx.x / K; slot < a.n;
+       slot += (long long)gridDim.x * kGroups)
+    detail::eval_slot<N, K>(src, T, a, slot, lane, gmask, tab);
+}
+
+static __global__ void __launch_bounds__(256) k_partials(EngineArgs a) {
+  const long long nchunk = (a.n + 31) / 32;
+  for (long long c = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / 32; c < nchunk;
+       c += (long long)gridDim.x * blockDim.x / 32)
+    detail::chunk_partial_warp(a, c, threadIdx.x & 31);
+}
+
+static __global__ void __launch_bounds__(256) k_decide(EngineArgs a) {
+  for (int k = (blockIdx.x * blockDim.x + threadIdx.x) / 32; k < a.nint;
+       k += gridDim.x * blockDim.x / 32)
+    detail::decide_warp(a, k, threadIdx.x & 31);
+}
+
+static __global__ void k_scan(EngineArgs a) {
+  detail::scan_warp(a, a.ctl->host.n_left, &a.ctl->host, threadIdx.x & 31);
+}
+
+template <int N>
+__global__ void __launch_bounds__(256) k_split(EngineArgs a) {
+  if (a.ctl->host.overflow) return;
+  const long long nchunk = (a.n + 31) / 32;
+  const long long gwarp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / 32;
+  const long long nwarp = (long long)gridDim.x * blockDim.x / 32;
+  for (long long c = gwarp; c < nchunk; c += nwarp) detail::split_chunk_warp<N>(a, c, threadIdx.x & 31);
+}
+
 static __global__ void k_advance(EngineArgs a) {
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < a.nint; k += gridDim.x * blockDim.x) {
-    IntegralState& is = a.ist[k];
-    if (is.state == kStateRunning) {
-      is.seg_start = is.next_start;
-      is.seg_count = is.next_count;
-      if (is.next_count == 0) is.state = kStateDone;
-    } else {
-      is.seg_count = 0;
-    }
-  }
+  if (a.ctl->host.overflow) return;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < a.nint; k += gridDim.x * blockDim.x)
+    detail::finish_integral(a, k);
   if (blockIdx.x == 0 && threadIdx.x == 0) {
-    a.ctl->n_cur = a.ctl->n_next;
-    a.ctl->iter += 1;
+    a.ctl->cur ^= 1;
+    a.ctl->iters_done += 1;
   }
 }
 

@@ -26,6 +26,9 @@ Options to_options(const cub_options* opt) {
   if (opt->phase2_max_regions > 0) o.phase2_max_regions = opt->phase2_max_regions;
   if (opt->max_slots > 0) o.max_slots = opt->max_slots;
   o.lanes = opt->lanes;
+  o.persistent = opt->no_persistent ? 0 : 1;
+  if (opt->persistent_max_n > 0) o.persistent_max_n = opt->persistent_max_n;
+  if (opt->persistent_block_n > 0) o.persistent_block_n = opt->persistent_block_n;
   return o;
 }
 
@@ -102,6 +105,9 @@ void cub_default_options(cub_options* opt) {
   opt->phase2_max_regions = o.phase2_max_regions;
   opt->max_slots = o.max_slots;
   opt->lanes = o.lanes;
+  opt->no_persistent = o.persistent ? 0 : 1;
+  opt->persistent_max_n = o.persistent_max_n;
+  opt->persistent_block_n = o.persistent_block_n;
 }
 
 cub_ctx* cub_create(int device) {
@@ -159,7 +165,20 @@ int cub_ctx_stats(const cub_ctx* ctx, cub_stats* out) {
   out->phase2_boxes = s.phase2_boxes;
   out->h2d_bytes = s.h2d_bytes;
   out->d2h_bytes = s.d2h_bytes;
+  out->ms_persistent = s.ms_persistent;
+  out->persistent_launches = s.persistent_launches;
+  out->persistent_iterations = s.persistent_iterations;
   return 0;
+}
+
+void cub_ctx_release(cub_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  ctx->ws->release();
+  if (ctx->d_params) cudaFree(ctx->d_params);
+  ctx->d_params = nullptr;
+  ctx->params_cap = 0;
 }
 
 void cub_ctx_reset_stats(cub_ctx* ctx) {
@@ -210,10 +229,29 @@ int cub_integrate_batch(cub_ctx* ctx, int family, int ndim, int count,
   }
   const Options o = to_options(opt);
   std::vector<Result> res(count);
-  const int rc = dispatch_run(ctx, family, ndim, count, h, d, er.data(), ea.data(), o, res.data());
+  // Under the reference policy an integral's list never exceeds its phase-1
+  // cap, so groups of max_slots / (2 cap + 96) integrals always fit (the
+  // driver needs room for 2 n + 32 per integral); larger batches run as a
+  // sequence of such groups.
+  int group = count;
+  if (o.policy == kPolicyReference && o.phase1_cap > 0) {
+    const long long per = 2ll * o.phase1_cap + 96;
+    group = (int)std::max<long long>(1, std::min<long long>(count, o.max_slots / per));
+  }
+  int rc = 0;
+  for (int g0 = 0; g0 < count && (rc == 0 || rc == kErrCapacity); g0 += group) {
+    const int gn = std::min(group, count - g0);
+    const int r = dispatch_run(ctx, family, ndim, gn, h + g0, d ? d + g0 : nullptr,
+                               er.data() + g0, ea.data() + g0, o, res.data() + g0);
+    if (r != 0) rc = r;
+  }
   if (rc == kErrCuda) {
     set_error(ctx->ws->error());
     return CUB_ERR_CUDA;
+  }
+  if (rc == kErrTimeout) {
+    set_error("a device-side grid barrier wait ran out (persistent kernel)");
+    return CUB_ERR_TIMEOUT;
   }
   if (rc == kErrCapacity) set_error("region capacity exceeded; results are the last estimates");
   if (rc < 0 && rc != kErrCapacity) return rc;

@@ -39,7 +39,7 @@ FAMILIES = {
 POLICY_REFERENCE = 0
 POLICY_BREADTH = 1
 
-ERR_INVALID, ERR_CUDA, ERR_CAPACITY, ERR_UNSUPPORTED = -1, -2, -3, -4
+ERR_INVALID, ERR_CUDA, ERR_CAPACITY, ERR_UNSUPPORTED, ERR_TIMEOUT = -1, -2, -3, -4, -5
 
 
 class CubatureError(RuntimeError):
@@ -78,6 +78,9 @@ class CStats(C.Structure):
         ("phase2_boxes", C.c_longlong),
         ("h2d_bytes", C.c_longlong),
         ("d2h_bytes", C.c_longlong),
+        ("ms_persistent", C.c_double),
+        ("persistent_launches", C.c_longlong),
+        ("persistent_iterations", C.c_longlong),
     ]
 
     def as_dict(self) -> dict:
@@ -92,7 +95,9 @@ class COptions(C.Structure):
         ("phase2_max_regions", C.c_int),
         ("max_slots", C.c_longlong),
         ("lanes", C.c_int),
-        ("reserved", C.c_int),
+        ("no_persistent", C.c_int),
+        ("persistent_max_n", C.c_int),
+        ("persistent_block_n", C.c_int),
     ]
 
 
@@ -102,6 +107,7 @@ EXPORTS = (
     "cub_ctx_bytes", "cub_integrate", "cub_integrate_batch", "cub_rule_tables", "cub_rule_eval",
     "cub_split_scratch_bytes", "cub_reduce_scratch_bytes", "cub_split", "cub_reduce",
     "cub_ctx_stream", "cub_ctx_stats", "cub_ctx_reset_stats", "cub_ctx_set_timing",
+    "cub_ctx_release",
 )
 
 _lib = None
@@ -135,6 +141,7 @@ def load_library(path: str | Path | None = None):
     L.cub_ctx_stats.argtypes = [vp, C.POINTER(CStats)]
     L.cub_ctx_reset_stats.argtypes = [vp]
     L.cub_ctx_set_timing.argtypes = [vp, C.c_int]
+    L.cub_ctx_release.argtypes = [vp]
     L.cub_rule_tables.argtypes = [C.c_int, dp, dp, dp, ip]
     L.cub_rule_eval.argtypes = [C.c_int, C.c_int, C.POINTER(GenzParams), C.c_longlong, vp, vp,
                                 C.c_longlong, C.c_double, C.c_double, vp, vp, vp, vp, vp]
@@ -219,7 +226,9 @@ class Result:
 
 
 def options(policy: int = POLICY_REFERENCE, phase1_cap: int = 0, max_iters: int = 0,
-            phase2_max_regions: int = 0, max_slots: int = 0, lanes: int = 0) -> COptions:
+            phase2_max_regions: int = 0, max_slots: int = 0, lanes: int = 0,
+            persistent: bool = True, persistent_max_n: int = 0,
+            persistent_block_n: int = 0) -> COptions:
     o = COptions()
     load_library().cub_default_options(C.byref(o))
     o.policy = policy
@@ -232,6 +241,11 @@ def options(policy: int = POLICY_REFERENCE, phase1_cap: int = 0, max_iters: int 
     if max_slots:
         o.max_slots = max_slots
     o.lanes = lanes
+    o.no_persistent = 0 if persistent else 1
+    if persistent_max_n:
+        o.persistent_max_n = persistent_max_n
+    if persistent_block_n:
+        o.persistent_block_n = persistent_block_n
     return o
 
 
@@ -285,6 +299,10 @@ class Context:
 
     def set_timing(self, on: bool):
         self._lib.cub_ctx_set_timing(self._h, 1 if on else 0)
+
+    def release(self):
+        """Return the device pools (they are reserved again on demand)."""
+        self._lib.cub_ctx_release(self._h)
 
     def integrate(self, f: Integrand, epsrel: float, epsabs: float,
                   opts: COptions | None = None) -> Result:

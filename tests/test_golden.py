@@ -90,17 +90,70 @@ def integrate_cases():
     return json.loads(INTEGRATE.read_text())
 
 
-@pytest.mark.parametrize("rec", integrate_cases(), ids=lambda r: r["name"])
+def phase2_case(rec):
+    return "phase2" in rec["name"]
+
+
+@pytest.mark.parametrize("rec", [r for r in integrate_cases() if not phase2_case(r)],
+                         ids=lambda r: r["name"])
 def test_oracle_matches_reference_integrate(oracle, rec):
-    """Full two-phase runs: value within 2 epsrel, same status, region counts
-    close (the reference's phase 2 keeps an approximate top-64 pool once a
-    box has 128 subregions, the oracle the exact maximum)."""
+    """Runs that finish in the first phase: the oracle reproduces the
+    reference's region count exactly, its status, and its value to rounding
+    (including the reference's per-region epsabs test, which can report
+    status 0 with an error estimate above the tolerance, case
+    cornerpeak6_epsabs)."""
     n = rec["ndim"]
     f = oracle.make_integrand(rec["family_name"], n, rec["a"], rec["u"])
     r = oracle.Rule(n).integrate_reference(f, rec["epsrel"], rec["epsabs"])
-    assert abs(r["value"] - rec["integral"]) <= 2 * rec["epsrel"] * abs(rec["integral"]) + 1e-15
-    if rec["errorFlag"] == 0:
-        assert r["status"] == 0
+    assert r["phase2_regions"] == 0
+    assert r["nregions"] == rec["nregions"]
+    assert r["neval"] == rec["neval"]
+    assert r["status"] == rec["errorFlag"]
+    assert abs(r["value"] - rec["integral"]) <= 1e-13 * abs(rec["integral"])
+    # the null rules difference nearly equal sums: compare on the value scale
+    assert abs(r["error"] - rec["error"]) <= 1e-13 * abs(rec["integral"]) + 1e-6 * rec["error"]
+
+
+@pytest.mark.parametrize("rec", [r for r in integrate_cases() if phase2_case(r)],
+                         ids=lambda r: r["name"])
+def test_reference_phase2_deviation(oracle, rec):
+    """Runs that reach the second phase.  The reference keeps up to 128
+    subregions of a leftover box in shared memory and, once full, spills to
+    a device-malloc'ed pool and pulls back an approximate top 64
+    (GPUQuadPhases.cu:184-420); on these golden cases its value moves away
+    from the analytic integral by far more than its own error estimate.  The
+    oracle refines the exact maximum-error subregion: same failed-box count
+    and region count within 0.2%, and a value within its estimate."""
+    n = rec["ndim"]
+    f = oracle.make_integrand(rec["family_name"], n, rec["a"], rec["u"])
+    r = oracle.Rule(n).integrate_reference(f, rec["epsrel"], rec["epsabs"])
+    exact = oracle.exact(f)
+    assert r["phase2_regions"] > 0
+    assert r["status"] == rec["errorFlag"]
+    assert abs(r["nregions"] - rec["nregions"]) <= 2e-3 * rec["nregions"]
+    ours = abs(r["value"] - exact)
+    theirs = abs(rec["integral"] - exact)
+    assert ours <= max(r["error"], rec["epsrel"] * abs(exact))
+    assert theirs > 10 * rec["error"]  # the documented deviation
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("rec", integrate_cases(), ids=lambda r: r["name"])
+def test_cuda_integrate_vs_reference(cub, oracle, ctx, rec):
+    """The CUDA engine against the reference engine's own integrate():
+    first-phase runs agree in status, region count (within 1%: the engines
+    sum the rule in different orders, so near-ties can flip) and value
+    (within 2 epsrel); second-phase runs agree in status and land within
+    their error estimate of the analytic value (where the reference does
+    not, see test_reference_phase2_deviation)."""
+    n = rec["ndim"]
+    r = ctx.integrate(cub.Integrand(rec["family_name"], n, rec["a"], rec["u"]), rec["epsrel"],
+                      rec["epsabs"])
+    exact = oracle.exact(oracle.make_integrand(rec["family_name"], n, rec["a"], rec["u"]))
+    assert r.status == rec["errorFlag"]
+    if not phase2_case(rec):
+        assert abs(r.nregions - rec["nregions"]) <= 0.01 * rec["nregions"]
+        assert abs(r.integral - rec["integral"]) <= 2 * rec["epsrel"] * abs(rec["integral"])
     else:
-        assert r["status"] > 0
-    assert abs(r["nregions"] - rec["nregions"]) <= 0.05 * rec["nregions"] + 4
+        assert abs(r.nregions - rec["nregions"]) <= 5e-3 * rec["nregions"]
+        assert abs(r.integral - exact) <= max(r.error, rec["epsrel"] * abs(exact))

@@ -14,6 +14,7 @@ Tolerances (FP64 throughout):
     their error estimates of the analytic value; region counts within 2%.
 """
 import math
+import zlib
 
 import numpy as np
 import pytest
@@ -50,14 +51,23 @@ def refined_list(oracle, n, rounds, seed, frac=0.5):
     return np.ascontiguousarray(lo), np.ascontiguousarray(ln)
 
 
+def assert_within(got, want, bound, label):
+    """Element-wise |got - want| <= bound, reporting the worst region."""
+    bad = ~(np.abs(got - want) <= bound)
+    if bad.any():
+        i = int(np.argmax(np.where(bad, np.abs(got - want) / np.maximum(bound, 1e-300), 0)))
+        raise AssertionError(f"{label}: {int(bad.sum())} regions out of tolerance; worst #{i}: "
+                             f"got {got[i]!r} want {want[i]!r} bound {bound[i]!r}")
+
+
 def compare_regions(o, g, label):
     avg_c, err_c, mag = o["avg"], o["err"], o["mag"]
     avg_g, err_g, ax_g, act_g = [t.cpu().numpy() for t in g]
     # rounding scale: |avg| plus the L1 magnitude of the rule sum (matters
     # where the integrand cancels over a region)
     scale = np.abs(avg_c) + mag
-    assert np.all(np.abs(avg_g - avg_c) <= 1e-13 * scale + 1e-300), label
-    assert np.all(np.abs(err_g - err_c) <= 1e-12 * scale + 1e-12 * err_c + 1e-300), label
+    assert_within(avg_g, avg_c, 1e-13 * scale + 1e-300, ("avg",) + tuple(label))
+    assert_within(err_g, err_c, 1e-12 * scale + 1e-12 * err_c + 1e-300, ("err",) + tuple(label))
     clear_axis = o["margin"] > 1e-9
     assert np.array_equal(ax_g[clear_axis], o["axis"][clear_axis]), label
     clear_ratio = np.abs(o["ratio"] - 1) > 1e-8
@@ -68,7 +78,7 @@ def compare_regions(o, g, label):
 @pytest.mark.parametrize("family", sorted(FAMILY_PARAMS))
 @pytest.mark.parametrize("n", [2, 3, 5, 8])
 def test_rule_eval_matches_oracle(cub, oracle, ctx, family, n):
-    rng = np.random.default_rng(hash((family, n)) % 2**32)
+    rng = np.random.default_rng(zlib.crc32(f"{family}-{n}".encode()))
     a, u = FAMILY_PARAMS[family](n, rng)
     rounds = {2: 6, 3: 5, 5: 4, 8: 2}[n]
     lo, ln = refined_list(oracle, n, rounds, seed=n)
@@ -256,3 +266,67 @@ def test_repeatable(cub, ctx):
     r1 = ctx.integrate(f, 1e-6, 1e-12)
     r2 = ctx.integrate(f, 1e-6, 1e-12)
     assert r1 == r2
+
+
+PERSIST_CASES = [
+    ("gaussian", 5, 5.0, 0.5, 1e-3),
+    ("corner_peak", 8, 0.5, 0.0, 1e-6),
+    ("product_peak", 4, [8.0, 12.0, 6.0, 10.0], [0.3, 0.6, 0.5, 0.4], 1e-5),
+    ("oscillatory", 3, [3.0, 2.0, 4.0], 0.2, 1e-8),
+]
+
+
+@pytest.mark.parametrize("family,n,a,u,epsrel", PERSIST_CASES)
+def test_persistent_matches_multilaunch(cub, oracle, ctx, family, n, a, u, epsrel):
+    """The persistent kernel (block- or warp-per-region evaluation, device-side
+    loop) and one launch per step agree."""
+    f = cub.Integrand(family, n, a, u)
+    rp = ctx.integrate(f, epsrel, 1e-12, cub.options(persistent=True))
+    rm = ctx.integrate(f, epsrel, 1e-12, cub.options(persistent=False))
+    assert rp.status == rm.status
+    assert abs(rp.integral - rm.integral) <= 1e-3 * epsrel * abs(rm.integral) + 1e-15
+    assert abs(rp.nregions - rm.nregions) <= 0.01 * rm.nregions + 4
+    ctx.reset_stats()
+    ctx.integrate(f, epsrel, 1e-12, cub.options(persistent=True))
+    st = ctx.stats()
+    assert st["persistent_launches"] >= 1
+
+
+def test_persistent_hands_over_and_back(cub, oracle, ctx):
+    """A small hand-over length makes the run alternate between the two
+    drivers; the result does not change."""
+    f = cub.Integrand("product_peak", 5, [20.0, 30.0, 10.0, 25.0, 15.0],
+                      [0.3, 0.5, 0.7, 0.45, 0.6])
+    ra = ctx.integrate(f, 1e-5, 1e-12, cub.options(persistent=False))
+    ctx.reset_stats()
+    rb = ctx.integrate(f, 1e-5, 1e-12, cub.options(persistent=True, persistent_max_n=256))
+    st = ctx.stats()
+    assert st["persistent_launches"] >= 1 and st["eval_launches"] >= 1
+    assert rb.status == ra.status
+    assert abs(rb.integral - ra.integral) <= 1e-8 * abs(ra.integral)
+    assert abs(rb.nregions - ra.nregions) <= 0.01 * ra.nregions + 4
+    fo = oracle.make_integrand("product_peak", 5, f.a, f.u)
+    assert abs(rb.integral - oracle.exact(fo)) <= 2e-5 * oracle.exact(fo)
+
+
+def test_persistent_batch(cub, oracle, ctx):
+    rng = np.random.default_rng(9)
+    n, eps = 6, 1e-4
+    params, refs = [], []
+    for k in range(7):
+        a = np.exp(rng.uniform(0, np.log(50), n))
+        u = rng.uniform(0.1, 0.9, n)
+        params.append(cub.make_params(n, list(a), list(u)))
+        refs.append(oracle.Rule(n).integrate_reference(
+            oracle.make_integrand("product_peak", n, a, u), eps, 1e-12))
+    rp = ctx.integrate_batch("product_peak", n, params, eps, 1e-12, cub.options(persistent=True))
+    rm = ctx.integrate_batch("product_peak", n, params, eps, 1e-12,
+                             cub.options(persistent=False))
+    for p, m, o in zip(rp, rm, refs):
+        # the reference algorithm's own answer (its error estimate can be
+        # optimistic for sharp peaks, so compare with the oracle, not the
+        # analytic value)
+        assert p.status == m.status == o["status"]
+        assert abs(p.integral - o["value"]) <= 1e-3 * eps * abs(o["value"])
+        assert abs(p.nregions - o["nregions"]) <= 0.01 * o["nregions"] + 4
+        assert abs(p.nregions - m.nregions) <= 0.01 * m.nregions + 4
