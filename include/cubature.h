@@ -204,6 +204,22 @@ int cub_split(int ndim, long long n, const double* d_lo, const double* d_len, lo
               long long out_ld, int layout, long long* d_count, void* d_scratch,
               size_t scratch_bytes, void* stream);
 
+/* cub_split for callers that cannot allocate device memory at call time
+ * (their memory belongs to another allocator, or a cudaMalloc/cudaFree --
+ * which can synchronise the device -- is not allowed on their path).  It
+ * allocates nothing: its scratch is a fixed 1 MiB device array in the
+ * library, so n is limited to 2^22 regions (larger n returns
+ * CUB_ERR_INVALID).  The array is shared by every call on a device: calls
+ * that overlap on the GPU race and must be serialised.  The first call on
+ * each device looks up the array's address; make it before any stream
+ * capture.  Same arguments and results as cub_split, minus the scratch.
+ * No counterpart in the reference (its GenerateActiveIntervals mallocs and
+ * frees its buffers on every iteration). */
+int cub_split_noalloc(int ndim, long long n, const double* d_lo, const double* d_len,
+                      long long ld, const int* d_active, const int* d_axis, double* d_out_lo,
+                      double* d_out_len, long long out_ld, int layout, long long* d_count,
+                      void* stream);
+
 /* The four sums of a phase-1 iteration (GPUKernelquad.cu:565-577):
  * d_out[0] = sum avg, [1] = sum err, [2] = sum avg over active == 0,
  * [3] = sum err over active == 0.  Device output; fixed-order tree. */

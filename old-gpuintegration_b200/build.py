@@ -52,7 +52,8 @@ def _stale(obj: Path, src: Path, deps: list[Path]) -> bool:
 
 
 def units() -> list[tuple[Path, Path, list[str]]]:
-    out = [(CSRC / "capi.cu", OBJ / "capi.o", [])]
+    out = [(CSRC / "capi.cu", OBJ / "capi.o", []),
+           (CSRC / "noalloc.cu", OBJ / "noalloc.o", [])]
     for n in DIMS:
         out.append((CSRC / "capi_dim.cu", OBJ / f"capi_dim{n}.o", [f"-DCUB_DIM={n}"]))
     return out

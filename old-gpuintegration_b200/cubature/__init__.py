@@ -107,7 +107,7 @@ EXPORTS = (
     "cub_ctx_bytes", "cub_integrate", "cub_integrate_batch", "cub_rule_tables", "cub_rule_eval",
     "cub_split_scratch_bytes", "cub_reduce_scratch_bytes", "cub_split", "cub_reduce",
     "cub_ctx_stream", "cub_ctx_stats", "cub_ctx_reset_stats", "cub_ctx_set_timing",
-    "cub_ctx_release",
+    "cub_ctx_release", "cub_split_noalloc",
 )
 
 _lib = None
@@ -152,6 +152,8 @@ def load_library(path: str | Path | None = None):
     L.cub_split.argtypes = [C.c_int, C.c_longlong, vp, vp, C.c_longlong, vp, vp, vp, vp,
                             C.c_longlong, C.c_int, vp, vp, C.c_size_t, vp]
     L.cub_reduce.argtypes = [C.c_longlong, vp, vp, vp, vp, vp, C.c_size_t, vp]
+    L.cub_split_noalloc.argtypes = [C.c_int, C.c_longlong, vp, vp, C.c_longlong, vp, vp, vp, vp,
+                                    C.c_longlong, C.c_int, vp, vp]
     if path is None:
         _lib = L
     return L
@@ -428,6 +430,26 @@ def split(lo, length, active, axis, layout: int = 0, stream=None):
     _check(L.cub_split(ndim, n, _ptr(lo), _ptr(length), n, _ptr(active), _ptr(axis), _ptr(olo),
                        _ptr(olen), cap, layout, _ptr(count), _ptr(scratch), scratch.numel(),
                        _stream_ptr(stream)))
+    m2 = int(count.item())
+    return olo[:, :m2].contiguous(), olen[:, :m2].contiguous()
+
+
+def split_noalloc(lo, length, active, axis, layout: int = 0, stream=None):
+    """split() through cub_split_noalloc: the library's fixed device scratch
+    instead of a caller buffer (at most 2^22 regions; calls must not overlap
+    on the GPU)."""
+    import torch
+
+    ndim, n = lo.shape
+    L = load_library()
+    dev = lo.device
+    count = torch.zeros(1, dtype=torch.int64, device=dev)
+    cap = max(2 * int(active.sum().item()), 1)
+    olo = torch.empty((ndim, cap), dtype=torch.float64, device=dev)
+    olen = torch.empty_like(olo)
+    _check(L.cub_split_noalloc(ndim, n, _ptr(lo), _ptr(length), n, _ptr(active), _ptr(axis),
+                               _ptr(olo), _ptr(olen), cap, layout, _ptr(count),
+                               _stream_ptr(stream)))
     m2 = int(count.item())
     return olo[:, :m2].contiguous(), olen[:, :m2].contiguous()
 
