@@ -94,16 +94,17 @@ typedef struct cub_options {
   int phase1_cap;          /* children that end phase 1 (default 16384)    */
   int max_iters;           /* breadth-first iteration limit (default 100)  */
   int phase2_max_regions;  /* bisections per leftover box (default 2048)   */
-  long long max_slots;     /* region-list capacity (default 2^26)          */
+  long long max_slots;     /* region-list capacity; 0 (default) = the
+                              slots that fit in 40% of free device memory */
   int lanes;               /* lanes per region in the multi-launch rule
                               kernel (1, 8 or 32); 0 = automatic          */
   int no_persistent;       /* 1: never use the persistent kernel           */
   int persistent_max_n;    /* list length above which the persistent
                               kernel hands over to one launch per step;
                               0 = automatic                               */
-  int persistent_block_n;  /* list length up to which the persistent kernel
-                              evaluates one region per block (else one per
-                              warp); 0 = automatic                        */
+  int persistent_max_r;    /* most regions a block of the persistent kernel
+                              evaluates at once (1, 2, 4 or 8; a region
+                              gets 256/R threads); 0 = 8                  */
 } cub_options;
 
 /* Library version, (major << 16) | minor. */
@@ -154,6 +155,14 @@ void cub_ctx_reset_stats(cub_ctx* ctx);
 /* Return the context's device pools to the driver (the next call reserves
  * what it needs again). */
 void cub_ctx_release(cub_ctx* ctx);
+
+/* Diagnostics: device timestamps (ns, %globaltimer) of the first 8
+ * iterations of the last persistent-kernel launch on this context, 8 per
+ * iteration: 0 start, 1 next segments assigned, 2 first grid barrier
+ * passed, 3 second grid barrier passed, 4 block 0's evaluations done,
+ * 5 last chunk summed, 6 integrals decided, 7 unused; zero where not
+ * reached.  out must hold 64 values. */
+int cub_ctx_trace(const cub_ctx* ctx, unsigned long long* out);
 void cub_ctx_set_timing(cub_ctx* ctx, int on);
 
 /* One integral over [0,1]^ndim: the body of GPUcuhre::integrate

@@ -39,11 +39,11 @@ struct Options {
   int phase1_cap = 1 << 14;       // FIRST_PHASE_MAXREGIONS (quad.h:21)
   int max_iters = 100;            // phase-1 iterations (GPUKernelquad.cu:631)
   int phase2_max_regions = 2048;  // MAX_GLOBALPOOL_SIZE (quad.h:9)
-  long long max_slots = 1ll << 26;
+  long long max_slots = 0;        // region-list capacity; 0 = from free device memory
   int lanes = 0;                  // lanes per region in the multi-launch rule kernel; 0 auto
   int persistent = 1;             // use the persistent kernel for short lists
   int persistent_max_n = 0;       // list length where it hands over; 0 auto
-  int persistent_block_n = 0;     // block-per-region evaluation up to this length; 0 auto
+  int persistent_max_r = 0;       // most regions per block in the persistent kernel (1,2,4,8); 0 = 8
 };
 
 struct Result {
@@ -91,6 +91,8 @@ inline const char* state_name(int s) {
   return "?";
 }
 
+inline long long auto_max_slots(int ndim, int policy);
+
 class Workspace {
  public:
   explicit Workspace(int device = 0) : device_(device) {}
@@ -125,6 +127,7 @@ class Workspace {
     cap_ = left_cap_ = 0;
     left_ndim_ = 0;
     heap_ints_ = 0;
+    for (auto& v : auto_slots_) v = 0;
     nint_cap_ = 0;
     slab_bytes_ = 0;
     ndim_ = 0;
@@ -163,8 +166,11 @@ class Workspace {
   long long left_cap() const { return left_cap_; }
 
   // Region lists for `slots` regions of dimension ndim; list `cur` keeps
-  // its first `keep` slots when the buffers grow.
-  bool reserve_lists(int ndim, long long slots, int cur, long long keep, cudaStream_t s) {
+  // its first `keep` slots when the buffers grow.  Growth doubles, capped at
+  // `limit` slots; everything but the preserved list is freed before the
+  // new buffers are allocated, so the peak is one old list plus the new set.
+  bool reserve_lists(int ndim, long long slots, int cur, long long keep, cudaStream_t s,
+                     long long limit = 1ll << 30) {
     if (slots <= cap_ && ndim == ndim_) return true;
     long long ncap;
     if (ndim != ndim_ || keep == 0) {
@@ -173,7 +179,18 @@ class Workspace {
       ncap = std::max<long long>(slots, 1 << 16);
     } else {
       ncap = std::max<long long>(slots, cap_ * 2);
+      free_buf(lo[cur ^ 1]);
+      free_buf(len[cur ^ 1]);
+      free_buf(rid[cur ^ 1]);
+      free_buf(avg);
+      free_buf(err);
+      free_buf(axis);
+      free_buf(active);
+      free_buf(part);
+      free_buf(chunk_excl);
+      free_buf(chunk_cnt);
     }
+    ncap = std::max<long long>(slots, std::min<long long>(ncap, limit));
     ncap = (ncap + 31) & ~31ll;
     double *nlo[2] = {nullptr, nullptr}, *nlen[2] = {nullptr, nullptr};
     int* nrid[2] = {nullptr, nullptr};
@@ -266,6 +283,15 @@ class Workspace {
     return true;
   }
 
+  // Automatic region capacity for (ndim, policy), measured once (free
+  // device memory) and kept until release().
+  long long auto_slots(int ndim, int policy) {
+    const int i = 2 * ndim + (policy == kPolicyReference ? 1 : 0);
+    if (ndim < 0 || ndim > kMaxDim) return auto_max_slots(ndim, policy);
+    if (!auto_slots_[i]) auto_slots_[i] = auto_max_slots(ndim, policy);
+    return auto_slots_[i];
+  }
+
   // Free the region lists and their per-slot scratch.
   void release_lists() {
     for (int b = 0; b < 2; ++b) {
@@ -350,6 +376,7 @@ class Workspace {
   }
 
   int device_;
+  long long auto_slots_[2 * (kMaxDim + 1)] = {};
   std::vector<std::pair<void*, size_t>> bufs_;
   long long cap_ = 0, left_cap_ = 0;
   int ndim_ = 0, left_ndim_ = 0;
@@ -364,6 +391,19 @@ inline int sm_count(int device) {
   int n = 0;
   cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, device);
   return n > 0 ? n : 148;
+}
+
+// Region-list capacity when the caller leaves it to the library: the slots
+// that fit in 40% of the device's free memory (two lists of FP64 bounds plus
+// per-slot results and chunk scratch, and leftover boxes under the reference
+// policy), between 2^20 and 2^30.
+inline long long auto_max_slots(int ndim, int policy) {
+  size_t free_b = 0, total_b = 0;
+  if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess || free_b == 0) return 1ll << 26;
+  double per_slot = 2.0 * (16.0 * ndim + 4) + 24 + 48.0 / 32;
+  if (policy == kPolicyReference) per_slot += 2.0 * (16.0 * ndim + 4 + 24);
+  const double slots = 0.4 * (double)free_b / per_slot;
+  return std::max<long long>(1ll << 20, std::min<long long>(1ll << 30, (long long)slots));
 }
 
 // Divisions per axis of the initial grid (GPUKernelquad.cu:300-311).
@@ -384,6 +424,7 @@ template <int N, class Src>
 int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
               const double* epsabs, const Options& opt, Result* out, cudaStream_t s) {
   static_assert(N >= 2 && N <= kMaxDim, "dimension out of range");
+  const long long max_slots = opt.max_slots > 0 ? opt.max_slots : ws.auto_slots(N, opt.policy);
   if (nint <= 0) return kErrInvalid;
   const RuleTables T = make_rule9_tables(N);
   const int sms = sm_count(ws.device());
@@ -395,7 +436,9 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
   Stats& st = ws.stats();
 
   if (!ws.reserve_integrals(nint, s)) return kErrCuda;
-  if (!ws.reserve_lists(N, std::max<long long>(1 << 20, 4 * n_cur), 0, 0, s)) return kErrCuda;
+  if (!ws.reserve_lists(N, std::min<long long>(std::max<long long>(1 << 20, 4 * n_cur), max_slots),
+                        0, 0, s, max_slots))
+    return kErrCuda;
   if (!ws.reserve_leftovers(N, 1, 0, s)) return kErrCuda;
 
   // integral states
@@ -461,14 +504,20 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
     st.launches += 1;
   }
 
-  // persistent kernel geometry
+  // persistent kernel geometry (queried once per device and instantiation)
   int pblocks = 0;
   if (opt.persistent) {
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_persistent<N, Src>, 256, 0);
-    int coop = 0;
-    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, ws.device());
-    if (per_sm > 0 && coop) pblocks = per_sm * sms;
+    static int per_sm_cache[64];
+    static bool cached[64];
+    const int dev = ws.device() & 63;
+    if (!cached[dev]) {
+      int per_sm = 0, coop = 0;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_persistent<N, Src>, 256, 0);
+      cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, ws.device());
+      per_sm_cache[dev] = coop ? per_sm : 0;
+      cached[dev] = true;
+    }
+    if (per_sm_cache[dev] > 0) pblocks = per_sm_cache[dev] * sms;
   }
   const int pmax = opt.persistent_max_n > 0 ? opt.persistent_max_n : pblocks * 8 * 8;
 
@@ -479,11 +528,13 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
     n_cur = hs.n;
     // capacity for the worst case of the coming iteration(s)
     const long long need = 2 * n_cur + 32ll * nint;
-    if (need > opt.max_slots) {
+    if (need > max_slots) {
       status = kErrCapacity;
       break;
     }
-    if (!ws.reserve_lists(N, std::max<long long>(need, 4 * n_cur), cur, n_cur, s)) return kErrCuda;
+    if (!ws.reserve_lists(N, std::min<long long>(std::max<long long>(need, 4 * n_cur), max_slots),
+                          cur, n_cur, s, max_slots))
+      return kErrCuda;
     if (opt.policy == kPolicyReference &&
         !ws.reserve_leftovers(N, n_left + 4 * n_cur + 1, n_left, s))
       return kErrCuda;
@@ -498,6 +549,7 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
       ws.ctl_host_->bar_count = 0;
       ws.ctl_host_->timeout = 0;
       ws.ctl_host_->exit_reason = 0;
+      std::memset(ws.ctl_host_->trace, 0, sizeof(ws.ctl_host_->trace));
       if (!ws.ck(cudaMemcpyAsync(ws.ctl, ws.ctl_host_, sizeof(Control), cudaMemcpyHostToDevice, s)))
         return kErrCuda;
       st.h2d_bytes += sizeof(Control);
@@ -509,10 +561,7 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
         p.rid[b] = ws.rid[b];
       }
       p.max_n = pmax;
-      // one region per block while every block gets at most one region;
-      // beyond that one region per warp keeps more points in flight
-      // (measured on B200: 8-D rule, 148 vs 1184 blocks' worth)
-      p.block_mode_max_n = opt.persistent_block_n > 0 ? opt.persistent_block_n : pblocks;
+      p.max_r = opt.persistent_max_r > 0 ? opt.persistent_max_r : 8;
       void* args[] = {(void*)&src, (void*)&T, (void*)&p};
       if (ws.timing) ws.ck(cudaEventRecord(ws.ev[0], s));
       if (!ws.ck(cudaLaunchCooperativeKernel((const void*)k_persistent<N, Src>, dim3(pblocks),

@@ -81,7 +81,25 @@ struct Control {
   unsigned bar_count;  // grid barrier arrivals
   unsigned bar_gen;    // grid barrier generation
   int timeout;         // a bounded wait gave up
+  // globaltimer stamps (ns) of the persistent kernel's first kTraceIters
+  // iterations, kTraceSlots per iteration (diagnostics, read back with the
+  // control block): 0 start, 1 scan done, 2 first barrier passed, 3 second
+  // barrier passed, 4 block 0's evaluations done, 5 last chunk complete,
+  // 6 integrals decided
+  unsigned long long trace[64];
 };
+constexpr int kTraceIters = 8;
+constexpr int kTraceSlots = 8;
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ void trace_mark(Control* ctl, int it, int slot) {
+  if (it < kTraceIters) ctl->trace[kTraceSlots * it + slot] = global_ns();
+}
 
 enum ExitReason : int {
   kExitDone = 1,      // no integral left running
@@ -430,7 +448,12 @@ __device__ __forceinline__ void finish_integral(const EngineArgs& a, int k) {
 // Multi-launch driver kernels (one launch per step).
 // ---------------------------------------------------------------------------
 template <int N, int K, class Src>
-__global__ void __launch_bounds__(256) k_eval(Src src, RuleTables T, EngineArgs a) {
+// Two blocks per SM (at most 128 registers): the rule kernel is bound by
+// FP64 latency, so warps in flight matter more than a few spilled values.
+#ifndef CUB_EVAL_MIN_BLOCKS
+#define CUB_EVAL_MIN_BLOCKS 2
+#endif
+__global__ void __launch_bounds__(256, CUB_EVAL_MIN_BLOCKS) k_eval(Src src, RuleTables T, EngineArgs a) {
   __shared__ detail::ItemTable<N> tab;
   if (threadIdx.x == 0) tab.fill();
   __syncthreads();

@@ -28,7 +28,7 @@ Options to_options(const cub_options* opt) {
   o.lanes = opt->lanes;
   o.persistent = opt->no_persistent ? 0 : 1;
   if (opt->persistent_max_n > 0) o.persistent_max_n = opt->persistent_max_n;
-  if (opt->persistent_block_n > 0) o.persistent_block_n = opt->persistent_block_n;
+  if (opt->persistent_max_r > 0) o.persistent_max_r = opt->persistent_max_r;
   return o;
 }
 
@@ -107,7 +107,7 @@ void cub_default_options(cub_options* opt) {
   opt->lanes = o.lanes;
   opt->no_persistent = o.persistent ? 0 : 1;
   opt->persistent_max_n = o.persistent_max_n;
-  opt->persistent_block_n = o.persistent_block_n;
+  opt->persistent_max_r = o.persistent_max_r;
 }
 
 cub_ctx* cub_create(int device) {
@@ -171,6 +171,16 @@ int cub_ctx_stats(const cub_ctx* ctx, cub_stats* out) {
   return 0;
 }
 
+int cub_ctx_trace(const cub_ctx* ctx, unsigned long long* out) {
+  if (!ctx || !out) {
+    set_error("invalid argument");
+    return CUB_ERR_INVALID;
+  }
+  const Control* c = ctx->ws->ctl_host_;
+  for (int i = 0; i < 64; ++i) out[i] = c ? c->trace[i] : 0;
+  return 0;
+}
+
 void cub_ctx_release(cub_ctx* ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
@@ -211,39 +221,73 @@ int cub_integrate_batch(cub_ctx* ctx, int family, int ndim, int count,
       return CUB_ERR_INVALID;
     }
   }
-  const GenzParams* d = nullptr;
-  if (count > 1) {
-    if (count > ctx->params_cap) {
-      if (ctx->d_params) cudaFree(ctx->d_params);
-      ctx->d_params = nullptr;
-      ctx->params_cap = 0;
-      if ((e = cudaMalloc(&ctx->d_params, sizeof(GenzParams) * count)) != cudaSuccess)
-        return cuda_fail(e, "cudaMalloc(params)");
-      ctx->params_cap = count;
-    }
-    if ((e = cudaMemcpyAsync(ctx->d_params, h, sizeof(GenzParams) * count,
-                             cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess)
-      return cuda_fail(e, "cudaMemcpyAsync(params)");
-    ctx->ws->stats().h2d_bytes += (long long)(sizeof(GenzParams) * count);
-    d = ctx->d_params;
+  if (count > 1 && count > ctx->params_cap) {
+    if (ctx->d_params) cudaFree(ctx->d_params);
+    ctx->d_params = nullptr;
+    ctx->params_cap = 0;
+    if ((e = cudaMalloc(&ctx->d_params, sizeof(GenzParams) * count)) != cudaSuccess)
+      return cuda_fail(e, "cudaMalloc(params)");
+    ctx->params_cap = count;
   }
-  const Options o = to_options(opt);
+  Options o = to_options(opt);
+  if (o.max_slots <= 0) o.max_slots = ctx->ws->auto_slots(ndim, o.policy);
   std::vector<Result> res(count);
-  // Under the reference policy an integral's list never exceeds its phase-1
-  // cap, so groups of max_slots / (2 cap + 96) integrals always fit (the
-  // driver needs room for 2 n + 32 per integral); larger batches run as a
-  // sequence of such groups.
+  // Groups of integrals that share one region list.  Under the reference
+  // policy an integral's list never exceeds its phase-1 cap, so groups of
+  // max_slots / (2 cap + 96) always fit (the driver needs room for 2 n + 32
+  // per integral).  Under the breadth policy lists are unbounded: the whole
+  // batch is tried at once and integrals that were still running when the
+  // capacity ran out are integrated again in groups a quarter the size
+  // (integrals are independent, so a rerun gives the same result).
   int group = count;
   if (o.policy == kPolicyReference && o.phase1_cap > 0) {
     const long long per = 2ll * o.phase1_cap + 96;
     group = (int)std::max<long long>(1, std::min<long long>(count, o.max_slots / per));
   }
+  std::vector<int> todo(count);
+  for (int k = 0; k < count; ++k) todo[k] = k;
+  std::vector<GenzParams> hp;
+  std::vector<double> ger, gea;
+  std::vector<Result> gres;
   int rc = 0;
-  for (int g0 = 0; g0 < count && (rc == 0 || rc == kErrCapacity); g0 += group) {
-    const int gn = std::min(group, count - g0);
-    const int r = dispatch_run(ctx, family, ndim, gn, h + g0, d ? d + g0 : nullptr,
-                               er.data() + g0, ea.data() + g0, o, res.data() + g0);
-    if (r != 0) rc = r;
+  while (!todo.empty()) {
+    std::vector<int> again;
+    for (size_t g0 = 0; g0 < todo.size(); g0 += group) {
+      const int gn = (int)std::min<size_t>(group, todo.size() - g0);
+      hp.resize(gn);
+      ger.resize(gn);
+      gea.resize(gn);
+      gres.assign(gn, Result());
+      for (int j = 0; j < gn; ++j) {
+        const int k = todo[g0 + j];
+        hp[j] = h[k];
+        ger[j] = er[k];
+        gea[j] = ea[k];
+      }
+      const GenzParams* d = nullptr;
+      if (gn > 1) {
+        if ((e = cudaMemcpyAsync(ctx->d_params, hp.data(), sizeof(GenzParams) * gn,
+                                 cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess)
+          return cuda_fail(e, "cudaMemcpyAsync(params)");
+        ctx->ws->stats().h2d_bytes += (long long)(sizeof(GenzParams) * gn);
+        d = ctx->d_params;
+      }
+      const int r = dispatch_run(ctx, family, ndim, gn, hp.data(), d, ger.data(), gea.data(), o,
+                                 gres.data());
+      if (r != 0 && r != kErrCapacity) {
+        rc = r;
+        break;
+      }
+      for (int j = 0; j < gn; ++j) {
+        const int k = todo[g0 + j];
+        res[k] = gres[j];
+        if (r == kErrCapacity && group > 1 && gres[j].state == kStateRunning) again.push_back(k);
+      }
+      if (r == kErrCapacity && (group == 1 || again.empty())) rc = kErrCapacity;
+    }
+    if (rc != 0 && rc != kErrCapacity) break;
+    todo.swap(again);
+    group = std::max(1, group / 4);
   }
   if (rc == kErrCuda) {
     set_error(ctx->ws->error());

@@ -97,7 +97,7 @@ class COptions(C.Structure):
         ("lanes", C.c_int),
         ("no_persistent", C.c_int),
         ("persistent_max_n", C.c_int),
-        ("persistent_block_n", C.c_int),
+        ("persistent_max_r", C.c_int),
     ]
 
 
@@ -107,7 +107,7 @@ EXPORTS = (
     "cub_ctx_bytes", "cub_integrate", "cub_integrate_batch", "cub_rule_tables", "cub_rule_eval",
     "cub_split_scratch_bytes", "cub_reduce_scratch_bytes", "cub_split", "cub_reduce",
     "cub_ctx_stream", "cub_ctx_stats", "cub_ctx_reset_stats", "cub_ctx_set_timing",
-    "cub_ctx_release", "cub_split_noalloc",
+    "cub_ctx_release", "cub_split_noalloc", "cub_ctx_trace",
 )
 
 _lib = None
@@ -142,6 +142,7 @@ def load_library(path: str | Path | None = None):
     L.cub_ctx_reset_stats.argtypes = [vp]
     L.cub_ctx_set_timing.argtypes = [vp, C.c_int]
     L.cub_ctx_release.argtypes = [vp]
+    L.cub_ctx_trace.argtypes = [vp, C.POINTER(C.c_ulonglong)]
     L.cub_rule_tables.argtypes = [C.c_int, dp, dp, dp, ip]
     L.cub_rule_eval.argtypes = [C.c_int, C.c_int, C.POINTER(GenzParams), C.c_longlong, vp, vp,
                                 C.c_longlong, C.c_double, C.c_double, vp, vp, vp, vp, vp]
@@ -230,7 +231,7 @@ class Result:
 def options(policy: int = POLICY_REFERENCE, phase1_cap: int = 0, max_iters: int = 0,
             phase2_max_regions: int = 0, max_slots: int = 0, lanes: int = 0,
             persistent: bool = True, persistent_max_n: int = 0,
-            persistent_block_n: int = 0) -> COptions:
+            persistent_max_r: int = 0) -> COptions:
     o = COptions()
     load_library().cub_default_options(C.byref(o))
     o.policy = policy
@@ -246,8 +247,8 @@ def options(policy: int = POLICY_REFERENCE, phase1_cap: int = 0, max_iters: int 
     o.no_persistent = 0 if persistent else 1
     if persistent_max_n:
         o.persistent_max_n = persistent_max_n
-    if persistent_block_n:
-        o.persistent_block_n = persistent_block_n
+    if persistent_max_r:
+        o.persistent_max_r = persistent_max_r
     return o
 
 
@@ -305,6 +306,15 @@ class Context:
     def release(self):
         """Return the device pools (they are reserved again on demand)."""
         self._lib.cub_ctx_release(self._h)
+
+    def trace(self) -> list[tuple[int, ...]]:
+        """Per-iteration device timestamps (ns) of the last persistent
+        launch, first 8 iterations, 8 per iteration: (start, segments
+        assigned, barrier 1, barrier 2, block 0 evaluated, last chunk
+        summed, integrals decided, unused)."""
+        buf = (C.c_ulonglong * 64)()
+        _check(self._lib.cub_ctx_trace(self._h, buf))
+        return [tuple(buf[8 * i + j] for j in range(8)) for i in range(8)]
 
     def integrate(self, f: Integrand, epsrel: float, epsabs: float,
                   opts: COptions | None = None) -> Result:
