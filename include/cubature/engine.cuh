@@ -149,6 +149,11 @@ class Workspace {
   ChunkPartial* part = nullptr;
   int* chunk_excl = nullptr;
   unsigned* chunk_cnt = nullptr;
+  // second parity of the persistent kernel's lazy split
+  int* axis_alt = nullptr;
+  int* excl_alt = nullptr;
+  unsigned* cmask = nullptr;  // two arrays of nchunk masks
+  int* chunk_int = nullptr;
   unsigned* int_cnt = nullptr;
   double* left_lo = nullptr;
   double* left_len = nullptr;
@@ -186,9 +191,7 @@ class Workspace {
       free_buf(err);
       free_buf(axis);
       free_buf(active);
-      free_buf(part);
-      free_buf(chunk_excl);
-      free_buf(chunk_cnt);
+      free_scratch();
     }
     ncap = std::max<long long>(slots, std::min<long long>(ncap, limit));
     ncap = (ncap + 31) & ~31ll;
@@ -220,18 +223,14 @@ class Workspace {
       len[b] = nlen[b];
       rid[b] = nrid[b];
     }
-    free_buf(avg);
-    free_buf(err);
-    free_buf(axis);
-    free_buf(active);
-    free_buf(part);
-    free_buf(chunk_excl);
-    free_buf(chunk_cnt);
+    free_scratch();
     const long long nchunk = ncap / 32 + 1;
     if (!alloc(&avg, sizeof(double) * ncap) || !alloc(&err, sizeof(double) * ncap) ||
         !alloc(&axis, sizeof(int) * ncap) || !alloc(&active, sizeof(int) * ncap) ||
         !alloc(&part, sizeof(ChunkPartial) * nchunk) || !alloc(&chunk_excl, sizeof(int) * nchunk) ||
-        !alloc(&chunk_cnt, sizeof(unsigned) * nchunk))
+        !alloc(&chunk_cnt, sizeof(unsigned) * nchunk) || !alloc(&axis_alt, sizeof(int) * ncap) ||
+        !alloc(&excl_alt, sizeof(int) * nchunk) || !alloc(&cmask, sizeof(unsigned) * 2 * nchunk) ||
+        !alloc(&chunk_int, sizeof(int) * nchunk))
       return false;
     if (!ck(cudaMemsetAsync(chunk_cnt, 0, sizeof(unsigned) * nchunk, s))) return false;
     cap_ = ncap;
@@ -299,6 +298,13 @@ class Workspace {
       free_buf(len[b]);
       free_buf(rid[b]);
     }
+    free_scratch();
+    cap_ = 0;
+    ndim_ = 0;
+  }
+
+  // Per-slot and per-chunk scratch of the lists.
+  void free_scratch() {
     free_buf(avg);
     free_buf(err);
     free_buf(axis);
@@ -306,8 +312,10 @@ class Workspace {
     free_buf(part);
     free_buf(chunk_excl);
     free_buf(chunk_cnt);
-    cap_ = 0;
-    ndim_ = 0;
+    free_buf(axis_alt);
+    free_buf(excl_alt);
+    free_buf(cmask);
+    free_buf(chunk_int);
   }
 
   bool reserve_integrals(int nint, cudaStream_t s) {
@@ -400,7 +408,7 @@ inline int sm_count(int device) {
 inline long long auto_max_slots(int ndim, int policy) {
   size_t free_b = 0, total_b = 0;
   if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess || free_b == 0) return 1ll << 26;
-  double per_slot = 2.0 * (16.0 * ndim + 4) + 24 + 48.0 / 32;
+  double per_slot = 2.0 * (16.0 * ndim + 4) + 28 + 64.0 / 32;
   if (policy == kPolicyReference) per_slot += 2.0 * (16.0 * ndim + 4 + 24);
   const double slots = 0.4 * (double)free_b / per_slot;
   return std::max<long long>(1ll << 20, std::min<long long>(1ll << 30, (long long)slots));
@@ -519,7 +527,8 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
     }
     if (per_sm_cache[dev] > 0) pblocks = per_sm_cache[dev] * sms;
   }
-  const int pmax = opt.persistent_max_n > 0 ? opt.persistent_max_n : pblocks * 8 * 8;
+  const int pmax = std::min(opt.persistent_max_n > 0 ? opt.persistent_max_n : pblocks * 8 * 8,
+                            32 * kStageChunks);
 
   IterState hs = c0.host;
   long long n_left = 0;
@@ -555,11 +564,19 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
       st.h2d_bytes += sizeof(Control);
       PersistArgs p;
       p.base = a;
+      const long long nchunk = ws.cap() / 32 + 1;
       for (int b = 0; b < 2; ++b) {
         p.lo[b] = ws.lo[b];
         p.len[b] = ws.len[b];
         p.rid[b] = ws.rid[b];
+        p.cmask[b] = ws.cmask + b * nchunk;
       }
+      p.axis[0] = ws.axis;
+      p.axis[1] = ws.axis_alt;
+      p.excl[0] = ws.chunk_excl;
+      p.excl[1] = ws.excl_alt;
+      p.chunk_int = ws.chunk_int;
+      p.iter_base = c0.iters_done;
       p.max_n = pmax;
       p.max_r = opt.persistent_max_r > 0 ? opt.persistent_max_r : 8;
       void* args[] = {(void*)&src, (void*)&T, (void*)&p};

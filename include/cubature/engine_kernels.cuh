@@ -53,12 +53,18 @@ struct IntegralState {
   int seg_start, seg_count;    // segment in the current list
   int next_start, next_count;  // segment in the next list
   int left_start, left_count;  // leftover boxes for phase 2
+  // persistent kernel, where the next list is built lazily: the segment
+  // of the list the current one was split from, and the global iteration
+  // whose first step copies this integral's leftovers (hand-off to phase 2)
+  int par_start, par_count;
+  int handoff_at, pad;
 };
 
 struct ChunkPartial {
   double sum_avg, sum_err;  // all regions of the chunk
   double fin_avg, fin_err;  // finished regions only
-  int nactive, pad;
+  int nactive;
+  unsigned mask;  // bit i: slot 32c + i stays active
 };
 
 // List sizes after one iteration's scan.
@@ -67,6 +73,7 @@ struct IterState {
   int n_running;  // integrals with regions in that list
   int n_left;     // leftover boxes queued for phase 2 so far
   int overflow;   // the list or the leftovers would exceed capacity
+  int handoff;    // some integral was handed to phase 2 by this scan
 };
 
 // Control block shared by the host and both drivers.
@@ -78,14 +85,13 @@ struct Control {
   int exit_reason;     // persistent kernel: why it returned
   int pad;
   unsigned done_cnt;   // integrals decided in this iteration
-  unsigned bar_count;  // grid barrier arrivals
-  unsigned bar_gen;    // grid barrier generation
+  unsigned bar_count;  // grid barrier arrivals since the launch (monotonic)
+  unsigned bar_gen;    // unused
   int timeout;         // a bounded wait gave up
   // globaltimer stamps (ns) of the persistent kernel's first kTraceIters
   // iterations, kTraceSlots per iteration (diagnostics, read back with the
-  // control block): 0 start, 1 scan done, 2 first barrier passed, 3 second
-  // barrier passed, 4 block 0's evaluations done, 5 last chunk complete,
-  // 6 integrals decided
+  // control block): 0 start, 1 next list assigned, 2 grid barrier passed,
+  // 4 block 0's evaluations done, 5 last chunk summed, 6 integrals decided
   unsigned long long trace[64];
 };
 constexpr int kTraceIters = 8;
@@ -123,6 +129,7 @@ struct EngineArgs {
   // chunk partials / prefix / arrival counters
   ChunkPartial* part;
   int* chunk_excl;
+  unsigned* cmask;  // active bit mask per chunk (optional)
   unsigned* chunk_cnt;
   unsigned* int_cnt;
   // next list
@@ -167,8 +174,8 @@ struct ParamSource {
 // Write one region's results (reference classification:
 // fail when err / max(epsrel|avg|, epsabs) > 1, GPUQuadPhases.cu:63-74).
 __device__ __forceinline__ void store_result(const EngineArgs& a, long long slot,
-                                             const RegionResult& r, const IntegralState& is) {
-  const double ratio = r.err / max_err(r.avg, is.epsrel, is.epsabs);
+                                             const RegionResult& r, double epsrel, double epsabs) {
+  const double ratio = r.err / max_err(r.avg, epsrel, epsabs);
   a.avg[slot] = r.avg;
   a.err[slot] = r.err;
   a.axis[slot] = r.axis;
@@ -207,7 +214,7 @@ __device__ __forceinline__ void eval_slot(const Src& src, const RuleTables& T,
     double jac = 1;
 #pragma unroll
     for (int d = 0; d < N; ++d) jac = __dmul_rn(jac, H[d]);
-    store_result(a, slot, finish_region<N>(rs, T, jac, 0), a.ist[k]);
+    store_result(a, slot, finish_region<N>(rs, T, jac, 0), a.ist[k].epsrel, a.ist[k].epsabs);
   }
 }
 
@@ -233,8 +240,54 @@ __device__ __forceinline__ void chunk_partial_warp(const EngineArgs& a, long lon
     p.fin_avg = s2;
     p.fin_err = s3;
     p.nactive = __popc(b);
-    p.pad = 0;
+    p.mask = b;
     a.part[c] = p;
+    if (a.cmask) a.cmask[c] = b;
+  }
+}
+
+// Stop decision for one running integral from the sums of its chunks and
+// its active-region count m (GPUKernelquad.cu:565-605).  Sets the child
+// count (next_count) or the leftover count (left_new) of phase 2.
+__device__ __forceinline__ void decide_integral(IntegralState& is, double s0, double s1, double s2,
+                                                double s3, int m, const EngineArgs& a) {
+  const double rG = is.value + s0, errG = is.error + s1;
+  is.value += s2;
+  is.error += s3;
+  is.last_value = rG;
+  is.last_error = errG;
+  is.nregions += (unsigned long long)is.seg_count;
+  is.neval += (unsigned long long)is.seg_count * (unsigned long long)a.npoints;
+  is.iters += 1;
+  is.next_count = 0;
+  is.left_new = 0;
+  if (errG <= max_err(rG, is.epsrel, is.epsabs)) {
+    // global stop test (GPUKernelquad.cu:583-598)
+    is.value = rG;
+    is.error = errG;
+    is.state = kStateDone;
+    is.status = 0;
+  } else if (m == 0) {
+    // every region finished on its own tolerance
+    is.state = kStateDone;
+    is.status = 0;
+  } else {
+    const long long children = 2ll * m;
+    const bool cap_hit = a.phase1_cap > 0 && children >= a.phase1_cap;
+    const bool iter_hit = is.iters >= a.max_iters;
+    if (cap_hit || iter_hit) {
+      if (a.policy == kPolicyReference) {
+        is.state = kStatePhase2;
+        is.left_new = (int)children;
+      } else {
+        is.state = kStateCapacity;
+        is.value = rG;
+        is.error = errG;
+        is.status = 1;
+      }
+    } else {
+      is.next_count = (int)children;
+    }
   }
 }
 
@@ -280,47 +333,7 @@ __device__ __forceinline__ void decide_warp(const EngineArgs& a, int k, int lane
     if (c < nc) a.chunk_excl[c0 + c] = running + incl - v;
     running += __shfl_sync(0xffffffffu, incl, 31);
   }
-  if (lane == 0) {
-    const int m = running;
-    const double rG = is.value + s0, errG = is.error + s1;
-    is.value += s2;
-    is.error += s3;
-    is.last_value = rG;
-    is.last_error = errG;
-    is.nregions += (unsigned long long)is.seg_count;
-    is.neval += (unsigned long long)is.seg_count * (unsigned long long)a.npoints;
-    is.iters += 1;
-    is.next_count = 0;
-    is.left_new = 0;
-    if (errG <= max_err(rG, is.epsrel, is.epsabs)) {
-      // global stop test (GPUKernelquad.cu:583-598)
-      is.value = rG;
-      is.error = errG;
-      is.state = kStateDone;
-      is.status = 0;
-    } else if (m == 0) {
-      // every region finished on its own tolerance
-      is.state = kStateDone;
-      is.status = 0;
-    } else {
-      const long long children = 2ll * m;
-      const bool cap_hit = a.phase1_cap > 0 && children >= a.phase1_cap;
-      const bool iter_hit = is.iters >= a.max_iters;
-      if (cap_hit || iter_hit) {
-        if (a.policy == kPolicyReference) {
-          is.state = kStatePhase2;
-          is.left_new = (int)children;
-        } else {
-          is.state = kStateCapacity;
-          is.value = rG;
-          is.error = errG;
-          is.status = 1;
-        }
-      } else {
-        is.next_count = (int)children;
-      }
-    }
-  }
+  if (lane == 0) decide_integral(is, s0, s1, s2, s3, running, a);
 }
 
 // A single warp assigns the next segments (32-aligned) and the leftover
@@ -365,6 +378,7 @@ __device__ __forceinline__ void scan_warp(const EngineArgs& a, int n_left_in, It
     s.n_running = nrun;
     s.n_left = carry_l;
     s.overflow = (carry_n > a.ncap) || (carry_l > a.left_cap);
+    s.handoff = 0;
     *out = s;
   }
 }

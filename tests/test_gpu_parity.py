@@ -330,3 +330,51 @@ def test_persistent_batch(cub, oracle, ctx):
         assert abs(p.integral - o["value"]) <= 1e-3 * eps * abs(o["value"])
         assert abs(p.nregions - o["nregions"]) <= 0.01 * o["nregions"] + 4
         assert abs(p.nregions - m.nregions) <= 0.01 * m.nregions + 4
+
+
+def _peak_batch(cub, n, count, seed):
+    rng = np.random.default_rng(seed)
+    params = []
+    for _ in range(count):
+        a = np.exp(rng.uniform(0, np.log(30), n))
+        u = rng.uniform(0.1, 0.9, n)
+        params.append(cub.make_params(n, list(a), list(u)))
+    return params
+
+
+@pytest.mark.parametrize("count", [5, 48])
+def test_persistent_batch_sizes(cub, ctx, count):
+    """Batches decided by one warp (up to 32 integrals) and integral by
+    integral (more than 32) give the answers of one launch per step."""
+    n, eps = 4, 1e-5
+    params = _peak_batch(cub, n, count, 21 + count)
+    ctx.reset_stats()
+    rp = ctx.integrate_batch("product_peak", n, params, eps, 1e-12, cub.options(persistent=True))
+    assert ctx.stats()["persistent_iterations"] >= 2
+    rm = ctx.integrate_batch("product_peak", n, params, eps, 1e-12,
+                             cub.options(persistent=False))
+    for p, m in zip(rp, rm):
+        assert p.status == m.status
+        assert abs(p.integral - m.integral) <= 1e-3 * eps * abs(m.integral) + 1e-15
+        assert abs(p.nregions - m.nregions) <= 0.01 * m.nregions + 4
+
+
+@pytest.mark.parametrize("count", [3, 40])
+def test_persistent_phase2_handoff(cub, ctx, count):
+    """Integrals handed to the depth-first phase inside the persistent kernel
+    get the same leftover boxes, hence the same results, as with one launch
+    per step."""
+    n, eps = 5, 1e-6
+    params = _peak_batch(cub, n, count, 5 + count)
+    opts = dict(phase1_cap=256)
+    ctx.reset_stats()
+    rp = ctx.integrate_batch("product_peak", n, params, eps, 1e-12,
+                             cub.options(persistent=True, **opts))
+    st = ctx.stats()
+    assert st["persistent_iterations"] >= 1 and st["phase2_boxes"] > 0
+    rm = ctx.integrate_batch("product_peak", n, params, eps, 1e-12,
+                             cub.options(persistent=False, **opts))
+    for p, m in zip(rp, rm):
+        assert p.status == m.status
+        assert abs(p.integral - m.integral) <= 1e-3 * eps * abs(m.integral) + 1e-15
+        assert abs(p.nregions - m.nregions) <= 0.01 * m.nregions + 4
