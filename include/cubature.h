@@ -158,10 +158,11 @@ void cub_ctx_release(cub_ctx* ctx);
 
 /* Diagnostics: device timestamps (ns, %globaltimer) of the first 8
  * iterations of the last persistent-kernel launch on this context, 8 per
- * iteration: 0 start, 1 next segments assigned, 2 first grid barrier
- * passed, 3 second grid barrier passed, 4 block 0's evaluations done,
- * 5 last chunk summed, 6 integrals decided, 7 unused; zero where not
- * reached.  out must hold 64 values. */
+ * iteration: 0 start, 1 next list assigned, 2 grid barrier passed,
+ * 3 deciding warp read its integral state, 4 block 0's evaluations done,
+ * 5 last chunk summed, 6 integrals decided, 7 chunk sums combined (3, 6
+ * and 7 for batches of up to 32 integrals); zero where not reached.  out
+ * must hold 64 values. */
 int cub_ctx_trace(const cub_ctx* ctx, unsigned long long* out);
 void cub_ctx_set_timing(cub_ctx* ctx, int on);
 
@@ -180,6 +181,22 @@ int cub_integrate_batch(cub_ctx* ctx, int family, int ndim, int count,
                         const cub_genz_params* params, const double* epsrel,
                         const double* epsabs, double epsrel0, double epsabs0,
                         const cub_options* opt, cub_result* out);
+
+/* cub_integrate over the box [lo, hi] (ndim values each, host memory,
+ * finite, hi > lo) instead of the unit cube: the reference's Volume
+ * argument (GPUQuadVolume.cu:4-25, GPUQuadSample.cu:44-56,174-179), here in
+ * FP64.  The initial grid is laid over the box, so every region is held in
+ * the integrand's own coordinates. */
+int cub_integrate_box(cub_ctx* ctx, int family, int ndim, const cub_genz_params* params,
+                      const double* lo, const double* hi, double epsrel, double epsabs,
+                      const cub_options* opt, cub_result* out);
+
+/* cub_integrate_batch with a box per integral: lo and hi are [count][ndim]
+ * host arrays. */
+int cub_integrate_batch_box(cub_ctx* ctx, int family, int ndim, int count,
+                            const cub_genz_params* params, const double* lo, const double* hi,
+                            const double* epsrel, const double* epsabs, double epsrel0,
+                            double epsabs0, const cub_options* opt, cub_result* out);
 
 /* ---- per-step entry points on caller device buffers ------------------ */
 

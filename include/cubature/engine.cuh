@@ -108,6 +108,8 @@ class Workspace {
     bytes_ = 0;
     if (ctl_host_) cudaFreeHost(ctl_host_);
     ctl_host_ = nullptr;
+    if (ist_host_) cudaFreeHost(ist_host_);
+    ist_host_ = nullptr;
     for (auto& e : ev) {
       if (e) cudaEventDestroy(e);
       e = nullptr;
@@ -117,6 +119,10 @@ class Workspace {
     axis = active = chunk_excl = nullptr;
     part = nullptr;
     chunk_cnt = int_cnt = nullptr;
+    axis_alt = excl_alt = chunk_int = nullptr;
+    cmask = nullptr;
+    box = nullptr;
+    box_cap_ = 0;
     left_lo = left_len = nullptr;
     left_rid = nullptr;
     left_res = nullptr;
@@ -154,6 +160,7 @@ class Workspace {
   int* excl_alt = nullptr;
   unsigned* cmask = nullptr;  // two arrays of nchunk masks
   int* chunk_int = nullptr;
+  double* box = nullptr;  // integration boxes of the current batch
   unsigned* int_cnt = nullptr;
   double* left_lo = nullptr;
   double* left_len = nullptr;
@@ -162,6 +169,7 @@ class Workspace {
   IntegralState* ist = nullptr;
   Control* ctl = nullptr;
   Control* ctl_host_ = nullptr;
+  IntegralState* ist_host_ = nullptr;  // pinned staging of the integral states
   void* slab = nullptr;
   int* heap = nullptr;
   int* counter = nullptr;
@@ -332,11 +340,24 @@ class Workspace {
     if (nint <= nint_cap_) return true;
     free_buf(ist);
     free_buf(int_cnt);
+    if (ist_host_) cudaFreeHost(ist_host_);
+    ist_host_ = nullptr;
+    nint_cap_ = 0;
     const int n = std::max(nint, 64);
     if (!alloc(&ist, sizeof(IntegralState) * n) || !alloc(&int_cnt, sizeof(unsigned) * n))
       return false;
+    if (!ck(cudaMallocHost(&ist_host_, sizeof(IntegralState) * n))) return false;
     if (!ck(cudaMemsetAsync(int_cnt, 0, sizeof(unsigned) * n, s))) return false;
     nint_cap_ = n;
+    return true;
+  }
+
+  bool reserve_boxes(size_t doubles) {
+    if (doubles <= box_cap_) return true;
+    free_buf(box);
+    box_cap_ = 0;
+    if (!alloc(&box, sizeof(double) * doubles)) return false;
+    box_cap_ = doubles;
     return true;
   }
 
@@ -390,6 +411,7 @@ class Workspace {
   int ndim_ = 0, left_ndim_ = 0;
   int nint_cap_ = 0;
   size_t slab_bytes_ = 0, heap_ints_ = 0;
+  size_t box_cap_ = 0;
   size_t bytes_ = 0;
   std::string err_;
   Stats stats_;
@@ -426,15 +448,17 @@ inline void launch_eval(const Src& src, const RuleTables& T, const EngineArgs& a
   k_eval<N, K, Src><<<(unsigned)blocks, 256, 0, s>>>(src, T, a);
 }
 
-// Run one batch: `nint` integrals of one family and dimension N, all
-// starting from the unit cube.  Results go to out[0..nint).
+// Run one batch: `nint` integrals of one family and dimension N, each over
+// its box (h_box[k] = lo[N] then hi[N], host memory; the unit cube when
+// h_box is null).  Results go to out[0..nint).
 template <int N, class Src>
 int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
-              const double* epsabs, const Options& opt, Result* out, cudaStream_t s) {
+              const double* epsabs, const Options& opt, Result* out, cudaStream_t s,
+              const double* h_box = nullptr) {
   static_assert(N >= 2 && N <= kMaxDim, "dimension out of range");
   const long long max_slots = opt.max_slots > 0 ? opt.max_slots : ws.auto_slots(N, opt.policy);
   if (nint <= 0) return kErrInvalid;
-  const RuleTables T = make_rule9_tables(N);
+  static const RuleTables T = make_rule9_tables(N);
   const int sms = sm_count(ws.device());
   const int dv = grid_divisions(N);
   int per = 1;
@@ -450,7 +474,7 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
   if (!ws.reserve_leftovers(N, 1, 0, s)) return kErrCuda;
 
   // integral states
-  std::vector<IntegralState> h(nint);
+  IntegralState* h = ws.ist_host_;
   for (int k = 0; k < nint; ++k) {
     IntegralState& is = h[k];
     std::memset(&is, 0, sizeof(is));
@@ -460,8 +484,7 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
     is.seg_start = k * padded;
     is.seg_count = per;
   }
-  if (!ws.ck(cudaMemcpyAsync(ws.ist, h.data(), sizeof(IntegralState) * nint,
-                             cudaMemcpyHostToDevice, s)))
+  if (!ws.ck(cudaMemcpyAsync(ws.ist, h, sizeof(IntegralState) * nint, cudaMemcpyHostToDevice, s)))
     return kErrCuda;
   Control c0;
   std::memset(&c0, 0, sizeof(c0));
@@ -508,7 +531,17 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
   bind(n_cur);
   {
     const long long blocks = std::min<long long>((n_cur + 255) / 256, (long long)sms * 8);
-    k_init_grid<N><<<(unsigned)std::max<long long>(blocks, 1), 256, 0, s>>>(a, dv, per, padded);
+    const double* d_box = nullptr;
+    if (h_box) {
+      const size_t nb = (size_t)nint * 2 * N;
+      if (!ws.reserve_boxes(nb)) return kErrCuda;
+      if (!ws.ck(cudaMemcpyAsync(ws.box, h_box, sizeof(double) * nb, cudaMemcpyHostToDevice, s)))
+        return kErrCuda;
+      st.h2d_bytes += (long long)(sizeof(double) * nb);
+      d_box = ws.box;
+    }
+    k_init_grid<N><<<(unsigned)std::max<long long>(blocks, 1), 256, 0, s>>>(a, dv, per, padded,
+                                                                          d_box);
     st.launches += 1;
   }
 
@@ -532,6 +565,7 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
 
   IterState hs = c0.host;
   long long n_left = 0;
+  bool states_fresh = false;  // h holds the device states after the last kernel
   int status = kOk;
   while (hs.n_running > 0 && hs.n > 0) {
     n_cur = hs.n;
@@ -587,10 +621,15 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
       if (ws.timing) ws.ck(cudaEventRecord(ws.ev[1], s));
       st.launches += 1;
       st.persistent_launches += 1;
-      if (!ws.ck(cudaMemcpyAsync(ws.ctl_host_, ws.ctl, sizeof(Control), cudaMemcpyDeviceToHost, s)))
+      // the states come back with the control block: when the launch
+      // finished every integral, no further round trip is needed
+      if (!ws.ck(cudaMemcpyAsync(ws.ctl_host_, ws.ctl, sizeof(Control), cudaMemcpyDeviceToHost, s)) ||
+          !ws.ck(cudaMemcpyAsync(h, ws.ist, sizeof(IntegralState) * nint, cudaMemcpyDeviceToHost,
+                                 s)))
         return kErrCuda;
       if (!ws.ck(cudaStreamSynchronize(s))) return kErrCuda;
-      st.d2h_bytes += sizeof(Control);
+      st.d2h_bytes += (long long)(sizeof(Control) + sizeof(IntegralState) * nint);
+      states_fresh = true;
       if (ws.timing) {
         float ms = 0;
         cudaEventElapsedTime(&ms, ws.ev[0], ws.ev[1]);
@@ -612,6 +651,7 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
     }
 
     // one iteration, one launch per step
+    states_fresh = false;
     int K = opt.lanes;
     if (K <= 0) K = n_cur >= (long long)sms * 512 ? 1 : (n_cur >= (long long)sms * 64 ? 8 : 32);
     if (ws.timing) ws.ck(cudaEventRecord(ws.ev[0], s));
@@ -656,6 +696,7 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
 
   if (status == kOk && n_left > 0) {
     // phase 2 on the leftover boxes
+    states_fresh = false;
     int dev_blocks = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&dev_blocks, k_phase2<N, Src>, 128, 0);
     dev_blocks = std::max(1, dev_blocks);
@@ -687,11 +728,12 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
     st.launches += 2;
   }
 
-  if (!ws.ck(cudaMemcpyAsync(h.data(), ws.ist, sizeof(IntegralState) * nint,
-                             cudaMemcpyDeviceToHost, s)))
-    return kErrCuda;
-  st.d2h_bytes += (long long)(sizeof(IntegralState) * nint);
-  if (!ws.ck(cudaStreamSynchronize(s))) return kErrCuda;
+  if (!states_fresh) {
+    if (!ws.ck(cudaMemcpyAsync(h, ws.ist, sizeof(IntegralState) * nint, cudaMemcpyDeviceToHost, s)))
+      return kErrCuda;
+    st.d2h_bytes += (long long)(sizeof(IntegralState) * nint);
+    if (!ws.ck(cudaStreamSynchronize(s))) return kErrCuda;
+  }
   if (!ws.ck(cudaGetLastError())) return kErrCuda;
   if (ws.timing && status == kOk && n_left > 0) {
     float ms = 0;

@@ -91,7 +91,8 @@ struct Control {
   // globaltimer stamps (ns) of the persistent kernel's first kTraceIters
   // iterations, kTraceSlots per iteration (diagnostics, read back with the
   // control block): 0 start, 1 next list assigned, 2 grid barrier passed,
-  // 4 block 0's evaluations done, 5 last chunk summed, 6 integrals decided
+  // 3 decider read its integral state, 4 block 0's evaluations done, 5 last
+  // chunk summed, 6 integrals decided, 7 chunk sums combined
   unsigned long long trace[64];
 };
 constexpr int kTraceIters = 8;
@@ -516,12 +517,13 @@ static __global__ void k_advance(EngineArgs a) {
   }
 }
 
-// Initial grid for every integral: d^N equal boxes of the unit cube
-// (GPUKernelquad.cu:24-61,300-316), dimension 0 varying fastest.
+// Initial grid for every integral: d^N equal boxes of its integration box
+// (box[k] = lo[N] then hi[N]; the unit cube when box is null),
+// GPUKernelquad.cu:24-61,300-316, dimension 0 varying fastest.
 template <int N>
-__global__ void k_init_grid(EngineArgs a, int divisions, int per_integral, int padded) {
+__global__ void k_init_grid(EngineArgs a, int divisions, int per_integral, int padded,
+                            const double* box) {
   const long long total = (long long)a.nint * padded;
-  const double w = 1.0 / divisions;
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
        t += (long long)gridDim.x * blockDim.x) {
     const int k = (int)(t / padded);
@@ -531,11 +533,14 @@ __global__ void k_init_grid(EngineArgs a, int divisions, int per_integral, int p
       continue;
     }
     int rem = j;
+    const double* bx = box ? box + (long long)k * 2 * N : nullptr;
 #pragma unroll
     for (int d = 0; d < N; ++d) {
       const int id = rem % divisions;
       rem /= divisions;
-      const_cast<double*>(a.lo)[(long long)d * a.cap + t] = 0 + id * w;
+      const double blo = bx ? bx[d] : 0.0;
+      const double w = (bx ? bx[N + d] - bx[d] : 1.0) / divisions;
+      const_cast<double*>(a.lo)[(long long)d * a.cap + t] = blo + id * w;
       const_cast<double*>(a.len)[(long long)d * a.cap + t] = w;
     }
     const_cast<int*>(a.rid)[t] = k;

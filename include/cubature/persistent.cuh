@@ -97,17 +97,23 @@ __device__ __forceinline__ bool grid_barrier(Control* ctl, unsigned target) {
   return ok;
 }
 
-// Points of the rule, for evaluation with one thread per point: a 32-bit
-// descriptor per point of sets 0..7 (set | d1<<4 | d2<<8 | d3<<12 |
-// signs<<16), in the oracle's enumeration order; the 2^N points of set 8
-// follow, their index is the sign pattern.
+// Points of the rule, for evaluation with one thread per point, in the
+// oracle's enumeration order: sets 0..7 (decoded from the point index) then
+// the 2^N points of set 8 (index = sign pattern).  Each point is stored as
+// N 4-bit coefficient codes, so that its coordinates are
+// x_i = fma(ctab[code_i], H_i, L_i) -- the same arithmetic as the
+// structured evaluator: code 0 is the box centre (0.5), codes 1..10 are
+// 0.5 -/+ g for the generators a1, a2, a3, a4 and the corner value.
 template <int N>
 struct PointTable {
   static constexpr int kNonCube = 1 + 8 * N + 6 * N * (N - 1) + 4 * N * (N - 1) * (N - 2) / 3;
   static constexpr int kPoints = kNonCube + (1 << N);
-  uint32_t desc[kNonCube];
+  static_assert(N <= 8, "4-bit codes of N axes must fit 32 bits");
+  uint2 ent[kPoints];  // x: codes (axis i at bits 4i..4i+3), y: generator set
+  double ctab[16];
 
-  // Descriptor of point p, decoded from its index.
+  // Descriptor of non-corner point p decoded from its index:
+  // set | d1<<4 | d2<<8 | d3<<12 | signs<<16.
   __host__ __device__ static uint32_t decode(int p) {
     if (p == 0) return 0;
     int q = p - 1;
@@ -156,39 +162,40 @@ struct PointTable {
     return 7 | (d1 << 4) | (d2 << 8) | ((d2 + 1 + t) << 12) | (sg << 16);
   }
 
+  // Code of generator gi (0..3: a1..a4, 4: corner value) with sign `minus`.
+  __host__ __device__ static uint32_t code(int gi, bool minus) {
+    return 1u + 2u * (uint32_t)gi + (minus ? 1u : 0u);
+  }
+
+  // Codes and set of point p.
+  __host__ __device__ static uint2 entry(int p) {
+    uint32_t codes = 0;
+    if (p >= kNonCube) {
+      const int s = p - kNonCube;
+      for (int i = 0; i < N; ++i) codes |= code(4, (s >> i) & 1) << (4 * i);
+      return make_uint2(codes, 8u);
+    }
+    const uint32_t dsc = decode(p);
+    const int set = dsc & 15;
+    const int d1 = (dsc >> 4) & 15, d2 = (dsc >> 8) & 15, d3 = (dsc >> 12) & 15;
+    const int sg = dsc >> 16;
+    const int nz = set == 0 ? 0 : (set <= 4 ? 1 : (set <= 6 ? 2 : 3));
+    const int g1 = set == 2 ? 1 : (set == 3 ? 2 : (set == 4 ? 3 : 0));
+    const int g2 = set == 6 ? 1 : 0;
+    if (nz >= 1) codes |= code(g1, sg & 1) << (4 * d1);
+    if (nz >= 2) codes |= code(g2, sg & 2) << (4 * d2);
+    if (nz >= 3) codes |= code(0, sg & 4) << (4 * d3);
+    return make_uint2(codes, (uint32_t)set);
+  }
+
   __device__ void fill(int tid, int nthreads) {
-    for (int p = tid; p < kNonCube; p += nthreads) desc[p] = decode(p);
+    if (tid < 16) {
+      const double gen[5] = {kGenA1, kGenA2, kGenA3, kGenA4, kGenL};
+      ctab[tid] = tid == 0 ? 0.5 : (tid <= 10 ? coef(gen[(tid - 1) >> 1], (tid - 1) & 1) : 0.0);
+    }
+    for (int p = tid; p < kPoints; p += nthreads) ent[p] = entry(p);
   }
 };
-
-template <int N>
-__device__ __forceinline__ void point_coords(const PointTable<N>& pt, int p, const double (&L)[N],
-                                             const double (&H)[N], const double (&C)[N],
-                                             double (&x)[N], int& set) {
-  if (p >= PointTable<N>::kNonCube) {
-    const int s = p - PointTable<N>::kNonCube;
-    set = 8;
-#pragma unroll
-    for (int i = 0; i < N; ++i) x[i] = fma(coef(kGenL, (s >> i) & 1), H[i], L[i]);
-    return;
-  }
-  const uint32_t dsc = pt.desc[p];
-  set = dsc & 15;
-  const int d1 = (dsc >> 4) & 15, d2 = (dsc >> 8) & 15, d3 = (dsc >> 12) & 15;
-  const int sg = dsc >> 16;
-  const int nz = set == 0 ? 0 : (set <= 4 ? 1 : (set <= 6 ? 2 : 3));
-  const double g1 = set == 2 ? kGenA2 : (set == 3 ? kGenA3 : (set == 4 ? kGenA4 : kGenA1));
-  const double g2 = set == 6 ? kGenA2 : kGenA1;
-  const double v1 = fma(coef(g1, sg & 1), pick(H, d1), pick(L, d1));
-  const double v2 = fma(coef(g2, sg & 2), pick(H, d2), pick(L, d2));
-  const double v3 = fma(coef(kGenA1, sg & 4), pick(H, d3), pick(L, d3));
-#pragma unroll
-  for (int i = 0; i < N; ++i)
-    x[i] = (nz >= 1 && i == d1) ? v1
-           : (nz >= 2 && i == d2) ? v2
-           : (nz >= 3 && i == d3) ? v3
-                                  : C[i];
-}
 
 template <int N>
 struct GroupSmem {
@@ -218,34 +225,23 @@ __device__ __forceinline__ RegionResult eval_region_group(const F& f, const doub
                                                           bool active) {
   constexpr int W = G / 32;
   const int lane = t & 31, wid = threadIdx.x >> 5;
-  double C[N];
-#pragma unroll
-  for (int i = 0; i < N; ++i) C[i] = fma(0.5, H[i], L[i]);
   double S[kNumSets];
 #pragma unroll
   for (int k = 0; k < kNumSets; ++k) S[k] = 0;
-  // points are sorted by set, so a thread's sets never decrease: keep one
-  // running sum and flush it into S[set] when the set changes
-  double acc = 0;
-  int cur = 0;
+  // Branch-free body, two points in flight per thread.  A thread's points
+  // of one set are consecutive, so adding into S[set] directly gives the
+  // same sums as a running sum flushed at set changes.
+#pragma unroll 2
   for (int p = active ? t : PointTable<N>::kPoints; p < PointTable<N>::kPoints; p += G) {
+    const uint2 e = sm.pt.ent[p];
     double x[N];
-    int set;
-    point_coords<N>(sm.pt, p, L, H, C, x, set);
+#pragma unroll
+    for (int i = 0; i < N; ++i) x[i] = fma(sm.pt.ctab[(e.x >> (4 * i)) & 15u], H[i], L[i]);
     const double fx = f(x);
     if (p <= 4 * N) sm.fstage[g][p] = fx;
-    if (set != cur) {
 #pragma unroll
-      for (int k = 0; k < kNumSets; ++k)
-        if (k == cur) S[k] += acc;
-      acc = 0;
-      cur = set;
-    }
-    acc += fx;
+    for (int k = 0; k < kNumSets; ++k) S[k] += (e.y == (unsigned)k) ? fx : 0.0;
   }
-#pragma unroll
-  for (int k = 0; k < kNumSets; ++k)
-    if (k == cur) S[k] += acc;
 #pragma unroll
   for (int k = 0; k < kNumSets; ++k) {
     double v = S[k];
@@ -487,6 +483,7 @@ static __device__ __noinline__ void decide_scan_small(const EngineArgs& a, const
   const bool have = lane < nint;
   IntegralState& is = a.ist[have ? lane : 0];
   const bool run = have && is.state == kStateRunning;
+  if (lane == 0) trace_mark(a.ctl, it, 3);
   double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
   int m = 0;
   if (nint == 1) {
@@ -537,6 +534,7 @@ static __device__ __noinline__ void decide_scan_small(const EngineArgs& a, const
       m += pc.nactive;
     }
   }
+  if (lane == 0) trace_mark(a.ctl, it, 7);
   bool entered = false;
   if (run) {
     decide_integral(is, s0, s1, s2, s3, m, a);

@@ -1,5 +1,6 @@
 // capi.cu -- the C ABI (include/cubature.h): contexts, dispatch by
 // dimension and family, per-step entry points.
+#include <cmath>
 #include <cstring>
 #include <string>
 
@@ -58,15 +59,15 @@ int cuda_fail(cudaError_t e, const char* what) {
 
 int dispatch_run(cub_ctx* ctx, int family, int ndim, int count, const GenzParams* h,
                  const GenzParams* d, const double* er, const double* ea, const Options& o,
-                 Result* out) {
+                 Result* out, const double* box) {
   switch (ndim) {
-    case 2: return run_dim_2(ctx, family, count, h, d, er, ea, o, out);
-    case 3: return run_dim_3(ctx, family, count, h, d, er, ea, o, out);
-    case 4: return run_dim_4(ctx, family, count, h, d, er, ea, o, out);
-    case 5: return run_dim_5(ctx, family, count, h, d, er, ea, o, out);
-    case 6: return run_dim_6(ctx, family, count, h, d, er, ea, o, out);
-    case 7: return run_dim_7(ctx, family, count, h, d, er, ea, o, out);
-    case 8: return run_dim_8(ctx, family, count, h, d, er, ea, o, out);
+    case 2: return run_dim_2(ctx, family, count, h, d, er, ea, o, out, box);
+    case 3: return run_dim_3(ctx, family, count, h, d, er, ea, o, out, box);
+    case 4: return run_dim_4(ctx, family, count, h, d, er, ea, o, out, box);
+    case 5: return run_dim_5(ctx, family, count, h, d, er, ea, o, out, box);
+    case 6: return run_dim_6(ctx, family, count, h, d, er, ea, o, out, box);
+    case 7: return run_dim_7(ctx, family, count, h, d, er, ea, o, out, box);
+    case 8: return run_dim_8(ctx, family, count, h, d, er, ea, o, out, box);
   }
   return CUB_ERR_INVALID;
 }
@@ -199,15 +200,26 @@ void cub_ctx_set_timing(cub_ctx* ctx, int on) {
   if (ctx) ctx->ws->timing = on != 0;
 }
 
-int cub_integrate_batch(cub_ctx* ctx, int family, int ndim, int count,
-                        const cub_genz_params* params, const double* epsrel,
-                        const double* epsabs, double epsrel0, double epsabs0,
-                        const cub_options* opt, cub_result* out) {
-  if (!ctx || !params || !out || count <= 0) {
+namespace {
+
+// Shared body of the integrate entry points; lo/hi are [count][ndim] host
+// arrays (both null: the unit cube).
+int integrate_impl(cub_ctx* ctx, int family, int ndim, int count, const cub_genz_params* params,
+                   const double* lo, const double* hi, const double* epsrel,
+                   const double* epsabs, double epsrel0, double epsabs0, const cub_options* opt,
+                   cub_result* out) {
+  if (!ctx || !params || !out || count <= 0 || (!lo) != (!hi)) {
     set_error("invalid argument");
     return CUB_ERR_INVALID;
   }
   if (!check_ndim(ndim) || !check_family(family)) return CUB_ERR_INVALID;
+  if (lo) {
+    for (long long i = 0; i < (long long)count * ndim; ++i)
+      if (!(std::isfinite(lo[i]) && std::isfinite(hi[i]) && hi[i] > lo[i])) {
+        set_error("integration box needs finite bounds with hi > lo");
+        return CUB_ERR_INVALID;
+      }
+  }
   cudaError_t e = cudaSetDevice(ctx->device);
   if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
   static_assert(sizeof(cub_genz_params) == sizeof(GenzParams), "params layout");
@@ -247,7 +259,7 @@ int cub_integrate_batch(cub_ctx* ctx, int family, int ndim, int count,
   std::vector<int> todo(count);
   for (int k = 0; k < count; ++k) todo[k] = k;
   std::vector<GenzParams> hp;
-  std::vector<double> ger, gea;
+  std::vector<double> ger, gea, gbox;
   std::vector<Result> gres;
   int rc = 0;
   while (!todo.empty()) {
@@ -264,6 +276,17 @@ int cub_integrate_batch(cub_ctx* ctx, int family, int ndim, int count,
         ger[j] = er[k];
         gea[j] = ea[k];
       }
+      if (lo) {
+        // per integral: lo[ndim] then hi[ndim]
+        gbox.resize((size_t)gn * 2 * ndim);
+        for (int j = 0; j < gn; ++j) {
+          const int k = todo[g0 + j];
+          for (int d = 0; d < ndim; ++d) {
+            gbox[(size_t)j * 2 * ndim + d] = lo[(size_t)k * ndim + d];
+            gbox[(size_t)j * 2 * ndim + ndim + d] = hi[(size_t)k * ndim + d];
+          }
+        }
+      }
       const GenzParams* d = nullptr;
       if (gn > 1) {
         if ((e = cudaMemcpyAsync(ctx->d_params, hp.data(), sizeof(GenzParams) * gn,
@@ -273,7 +296,7 @@ int cub_integrate_batch(cub_ctx* ctx, int family, int ndim, int count,
         d = ctx->d_params;
       }
       const int r = dispatch_run(ctx, family, ndim, gn, hp.data(), d, ger.data(), gea.data(), o,
-                                 gres.data());
+                                 gres.data(), lo ? gbox.data() : nullptr);
       if (r != 0 && r != kErrCapacity) {
         rc = r;
         break;
@@ -303,10 +326,39 @@ int cub_integrate_batch(cub_ctx* ctx, int family, int ndim, int count,
   return rc == kErrCapacity ? CUB_ERR_CAPACITY : 0;
 }
 
+}  // namespace
+
+int cub_integrate_batch(cub_ctx* ctx, int family, int ndim, int count,
+                        const cub_genz_params* params, const double* epsrel,
+                        const double* epsabs, double epsrel0, double epsabs0,
+                        const cub_options* opt, cub_result* out) {
+  return integrate_impl(ctx, family, ndim, count, params, nullptr, nullptr, epsrel, epsabs,
+                        epsrel0, epsabs0, opt, out);
+}
+
+int cub_integrate_batch_box(cub_ctx* ctx, int family, int ndim, int count,
+                            const cub_genz_params* params, const double* lo, const double* hi,
+                            const double* epsrel, const double* epsabs, double epsrel0,
+                            double epsabs0, const cub_options* opt, cub_result* out) {
+  return integrate_impl(ctx, family, ndim, count, params, lo, hi, epsrel, epsabs, epsrel0,
+                        epsabs0, opt, out);
+}
+
 int cub_integrate(cub_ctx* ctx, int family, int ndim, const cub_genz_params* params,
                   double epsrel, double epsabs, const cub_options* opt, cub_result* out) {
-  return cub_integrate_batch(ctx, family, ndim, 1, params, nullptr, nullptr, epsrel, epsabs, opt,
-                             out);
+  return integrate_impl(ctx, family, ndim, 1, params, nullptr, nullptr, nullptr, nullptr, epsrel,
+                        epsabs, opt, out);
+}
+
+int cub_integrate_box(cub_ctx* ctx, int family, int ndim, const cub_genz_params* params,
+                      const double* lo, const double* hi, double epsrel, double epsabs,
+                      const cub_options* opt, cub_result* out) {
+  if (!lo || !hi) {
+    set_error("invalid argument: lo and hi are required");
+    return CUB_ERR_INVALID;
+  }
+  return integrate_impl(ctx, family, ndim, 1, params, lo, hi, nullptr, nullptr, epsrel, epsabs,
+                        opt, out);
 }
 
 int cub_rule_tables(int ndim, double* wt, double* scale, double* norm, int* count) {

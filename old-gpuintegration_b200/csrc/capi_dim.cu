@@ -18,13 +18,14 @@ constexpr int N = CUB_DIM;
 
 template <template <int> class Fam>
 int run_family(cub_ctx* ctx, int count, const GenzParams* h_params, const GenzParams* d_params,
-               const double* epsrel, const double* epsabs, const Options& opt, Result* out) {
+               const double* epsrel, const double* epsabs, const Options& opt, Result* out,
+               const double* h_box) {
   if (count == 1) {
     detail::SingleSource<Fam<N>> src{Fam<N>::load(h_params[0])};
-    return run_batch<N>(*ctx->ws, src, 1, epsrel, epsabs, opt, out, ctx->stream);
+    return run_batch<N>(*ctx->ws, src, 1, epsrel, epsabs, opt, out, ctx->stream, h_box);
   }
   detail::ParamSource<Fam<N>> src{d_params};
-  return run_batch<N>(*ctx->ws, src, count, epsrel, epsabs, opt, out, ctx->stream);
+  return run_batch<N>(*ctx->ws, src, count, epsrel, epsabs, opt, out, ctx->stream, h_box);
 }
 
 template <template <int> class Fam>
@@ -52,15 +53,16 @@ int rule_family(const GenzParams& p, long long n, const double* lo, const double
 
 int CUB_CAT(run_dim_, CUB_DIM)(cub_ctx* ctx, int family, int count, const GenzParams* h_params,
                                const GenzParams* d_params, const double* epsrel,
-                               const double* epsabs, const Options& opt, Result* out) {
+                               const double* epsabs, const Options& opt, Result* out,
+                               const double* h_box) {
   switch (family) {
-    case kGaussian: return run_family<Gaussian>(ctx, count, h_params, d_params, epsrel, epsabs, opt, out);
-    case kOscillatory: return run_family<Oscillatory>(ctx, count, h_params, d_params, epsrel, epsabs, opt, out);
-    case kCornerPeak: return run_family<CornerPeak>(ctx, count, h_params, d_params, epsrel, epsabs, opt, out);
-    case kProductPeak: return run_family<ProductPeak>(ctx, count, h_params, d_params, epsrel, epsabs, opt, out);
-    case kContinuous: return run_family<Continuous>(ctx, count, h_params, d_params, epsrel, epsabs, opt, out);
-    case kDiscontinuous: return run_family<Discontinuous>(ctx, count, h_params, d_params, epsrel, epsabs, opt, out);
-    case kCosSum: return run_family<CosSum>(ctx, count, h_params, d_params, epsrel, epsabs, opt, out);
+    case kGaussian: return run_family<Gaussian>(ctx, count, h_params, d_params, epsrel, epsabs, opt, out, h_box);
+    case kOscillatory: return run_family<Oscillatory>(ctx, count, h_params, d_params, epsrel, epsabs, opt, out, h_box);
+    case kCornerPeak: return run_family<CornerPeak>(ctx, count, h_params, d_params, epsrel, epsabs, opt, out, h_box);
+    case kProductPeak: return run_family<ProductPeak>(ctx, count, h_params, d_params, epsrel, epsabs, opt, out, h_box);
+    case kContinuous: return run_family<Continuous>(ctx, count, h_params, d_params, epsrel, epsabs, opt, out, h_box);
+    case kDiscontinuous: return run_family<Discontinuous>(ctx, count, h_params, d_params, epsrel, epsabs, opt, out, h_box);
+    case kCosSum: return run_family<CosSum>(ctx, count, h_params, d_params, epsrel, epsabs, opt, out, h_box);
   }
   return CUB_ERR_INVALID;
 }

@@ -28,7 +28,7 @@ Options to_options(const cub_options* opt);
 #define CUB_DECLARE_DIM(N)                                                                     \
   int run_dim_##N(cub_ctx* ctx, int family, int count, const GenzParams* h_params,             \
                   const GenzParams* d_params, const double* epsrel, const double* epsabs,      \
-                  const Options& opt, Result* out);                                            \
+                  const Options& opt, Result* out, const double* h_box);                       \
   int rule_eval_dim_##N(int family, const GenzParams& p, long long n, const double* lo,        \
                         const double* len, long long ld, double epsrel, double epsabs,         \
                         double* avg, double* err, int* axis, int* active, cudaStream_t s);     \

@@ -107,7 +107,8 @@ EXPORTS = (
     "cub_ctx_bytes", "cub_integrate", "cub_integrate_batch", "cub_rule_tables", "cub_rule_eval",
     "cub_split_scratch_bytes", "cub_reduce_scratch_bytes", "cub_split", "cub_reduce",
     "cub_ctx_stream", "cub_ctx_stats", "cub_ctx_reset_stats", "cub_ctx_set_timing",
-    "cub_ctx_release", "cub_split_noalloc", "cub_ctx_trace",
+    "cub_ctx_release", "cub_split_noalloc", "cub_ctx_trace", "cub_integrate_box",
+    "cub_integrate_batch_box",
 )
 
 _lib = None
@@ -136,6 +137,12 @@ def load_library(path: str | Path | None = None):
     L.cub_integrate_batch.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.POINTER(GenzParams), dp, dp,
                                       C.c_double, C.c_double, C.POINTER(COptions),
                                       C.POINTER(CResult)]
+    L.cub_integrate_box.argtypes = [vp, C.c_int, C.c_int, C.POINTER(GenzParams), dp, dp,
+                                    C.c_double, C.c_double, C.POINTER(COptions),
+                                    C.POINTER(CResult)]
+    L.cub_integrate_batch_box.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.POINTER(GenzParams),
+                                          dp, dp, dp, dp, C.c_double, C.c_double,
+                                          C.POINTER(COptions), C.POINTER(CResult)]
     L.cub_ctx_stream.argtypes = [vp]
     L.cub_ctx_stream.restype = vp
     L.cub_ctx_stats.argtypes = [vp, C.POINTER(CStats)]
@@ -317,15 +324,25 @@ class Context:
         return [tuple(buf[8 * i + j] for j in range(8)) for i in range(8)]
 
     def integrate(self, f: Integrand, epsrel: float, epsabs: float,
-                  opts: COptions | None = None) -> Result:
+                  opts: COptions | None = None, lo=None, hi=None) -> Result:
+        """One integral over [0,1]^n, or over the box [lo, hi] when given."""
         out = CResult()
         p = f.params()
-        _check(self._lib.cub_integrate(self._h, family_id(f.family), f.ndim, C.byref(p), epsrel,
-                                       epsabs, C.byref(opts) if opts else None, C.byref(out)))
+        o = C.byref(opts) if opts else None
+        if lo is None and hi is None:
+            _check(self._lib.cub_integrate(self._h, family_id(f.family), f.ndim, C.byref(p),
+                                           epsrel, epsabs, o, C.byref(out)))
+        else:
+            blo = (C.c_double * f.ndim)(*_axis_values(0.0 if lo is None else lo, f.ndim))
+            bhi = (C.c_double * f.ndim)(*_axis_values(1.0 if hi is None else hi, f.ndim))
+            _check(self._lib.cub_integrate_box(self._h, family_id(f.family), f.ndim, C.byref(p),
+                                               blo, bhi, epsrel, epsabs, o, C.byref(out)))
         return Result.from_c(out)
 
     def integrate_batch(self, family, ndim: int, params: Sequence[GenzParams], epsrel,
-                        epsabs, opts: COptions | None = None) -> list[Result]:
+                        epsabs, opts: COptions | None = None, lo=None, hi=None) -> list[Result]:
+        """Independent integrals on one region list; lo/hi (count x ndim)
+        give a box per integral."""
         n = len(params)
         arr = (GenzParams * n)(*params)
         out = (CResult * n)()
@@ -339,11 +356,30 @@ class Context:
             ea0 = float(epsabs)
         else:
             ea = (C.c_double * n)(*[float(x) for x in epsabs])
-        rc = self._lib.cub_integrate_batch(self._h, family_id(family), ndim, n, arr, er, ea, er0,
-                                           ea0, C.byref(opts) if opts else None, out)
+        o = C.byref(opts) if opts else None
+        if lo is None and hi is None:
+            rc = self._lib.cub_integrate_batch(self._h, family_id(family), ndim, n, arr, er, ea,
+                                               er0, ea0, o, out)
+        else:
+            blo = (C.c_double * (n * ndim))(*[v for k in range(n) for v in _axis_values(
+                0.0 if lo is None else lo[k], ndim)])
+            bhi = (C.c_double * (n * ndim))(*[v for k in range(n) for v in _axis_values(
+                1.0 if hi is None else hi[k], ndim)])
+            rc = self._lib.cub_integrate_batch_box(self._h, family_id(family), ndim, n, arr, blo,
+                                                   bhi, er, ea, er0, ea0, o, out)
         if rc < 0 and rc != ERR_CAPACITY:
             raise CubatureError(rc, last_error())
         return [Result.from_c(out[i]) for i in range(n)]
+
+
+def _axis_values(v, ndim: int) -> list[float]:
+    """A scalar or per-axis sequence as ndim floats."""
+    if isinstance(v, (int, float)):
+        return [float(v)] * ndim
+    v = [float(x) for x in v]
+    if len(v) != ndim:
+        raise ValueError("box bounds need one value per axis")
+    return v
 
 
 class GPUcuhre:
@@ -367,11 +403,14 @@ class GPUcuhre:
         self.num_devices = num_devices
         self.ctx = Context(device)
 
-    def integrate(self, f: Integrand, epsrel: float, epsabs: float,
+    def integrate(self, f: Integrand, epsrel: float, epsabs: float, vol=None,
                   policy: int = POLICY_REFERENCE, **kw) -> Result:
+        """vol = (lo, hi): the integration box, the reference's Volume
+        argument (GPUquad.h:611-620); None is the unit cube."""
         if f.ndim != self.ndim:
             raise ValueError("integrand dimension does not match the rule")
-        return self.ctx.integrate(f, epsrel, epsabs, options(policy=policy, **kw))
+        lo, hi = (None, None) if vol is None else vol
+        return self.ctx.integrate(f, epsrel, epsabs, options(policy=policy, **kw), lo=lo, hi=hi)
 
 
 def rule_tables(ndim: int):

@@ -299,6 +299,20 @@ double orc_eval_integrand(const orc_integrand* f, const double* x)
 double orc_exact(const orc_integrand* f)
 {
   const int n = f->ndim;
+  if (f->has_box) {
+    /* closed forms over a box for the separable families */
+    double p = 1;
+    for (int d = 0; d < n; ++d) {
+      const double a = f->a[d], u = f->u[d], l = f->box_lo[d], h = f->box_hi[d];
+      if (f->family == ORC_GAUSSIAN)
+        p *= sqrt(M_PI) / (2 * a) * (erf(a * (h - u)) - erf(a * (l - u)));
+      else if (f->family == ORC_PRODUCT_PEAK)
+        p *= a * (atan(a * (h - u)) - atan(a * (l - u)));
+      else
+        return NAN;
+    }
+    return p;
+  }
   switch (f->family) {
     case ORC_GAUSSIAN: {
       double p = 1;
@@ -543,6 +557,27 @@ size_t orc_initial_grid(int ndim, double* lo, double* len)
   return count;
 }
 
+size_t orc_initial_grid_box(const orc_integrand* f, double* lo, double* len)
+{
+  const int ndim = f->ndim;
+  if (!f->has_box) return orc_initial_grid(ndim, lo, len);
+  const int dv = grid_divisions(ndim);
+  size_t count = 1;
+  for (int d = 0; d < ndim; ++d) count *= (size_t)dv;
+  if (!lo) return count;
+  for (size_t i = 0; i < count; ++i) {
+    size_t rem = i;
+    for (int d = 0; d < ndim; ++d) {
+      const double w = (f->box_hi[d] - f->box_lo[d]) / dv;
+      size_t id = rem % (size_t)dv;
+      rem /= (size_t)dv;
+      lo[(size_t)d * count + i] = f->box_lo[d] + id * w;
+      len[(size_t)d * count + i] = w;
+    }
+  }
+  return count;
+}
+
 /* pairwise sum: the reductions only need to be accurate, not ordered */
 static double psum(const double* v, size_t n)
 {
@@ -675,10 +710,10 @@ int orc_integrate_reference(const orc_rule* r, const orc_integrand* f, double ep
   if (phase1_cap <= 0) phase1_cap = 1 << 14; /* FIRST_PHASE_MAXREGIONS, quad.h:21 */
   memset(out, 0, sizeof(*out));
 
-  size_t n = orc_initial_grid(nd, NULL, NULL);
+  size_t n = orc_initial_grid_box(f, NULL, NULL);
   double* lo = (double*)malloc(sizeof(double) * n * nd);
   double* len = (double*)malloc(sizeof(double) * n * nd);
-  orc_initial_grid(nd, lo, len);
+  orc_initial_grid_box(f, lo, len);
 
   double integral = 0, error = 0;
   size_t nregions = 0, neval = 0;
@@ -774,10 +809,10 @@ int orc_integrate_global(const orc_rule* r, const orc_integrand* f, double epsre
   const size_t fe = (size_t)r->npts;
   memset(out, 0, sizeof(*out));
   if (max_iters <= 0) max_iters = 200;
-  size_t n = orc_initial_grid(nd, NULL, NULL);
+  size_t n = orc_initial_grid_box(f, NULL, NULL);
   double* lo = (double*)malloc(sizeof(double) * n * nd);
   double* len = (double*)malloc(sizeof(double) * n * nd);
-  orc_initial_grid(nd, lo, len);
+  orc_initial_grid_box(f, lo, len);
   double fin_value = 0, fin_error = 0, estimate = 0;
   int have_estimate = 0, status = 1, iters = 0;
   size_t nregions = 0, neval = 0;
@@ -856,7 +891,10 @@ int orc_cuhre_sequential(const orc_rule* r, const orc_integrand* f, double epsre
   int hn = 0;
   size_t used = 0;
   double Lz[ORC_MAXDIM], W1[ORC_MAXDIM];
-  for (int d = 0; d < n; ++d) { Lz[d] = 0; W1[d] = 1; }
+  for (int d = 0; d < n; ++d) {
+    Lz[d] = f->has_box ? f->box_lo[d] : 0;
+    W1[d] = f->has_box ? f->box_hi[d] - f->box_lo[d] : 1;
+  }
   orc_result res;
   p2_region* r0 = &pool[used++];
   for (int d = 0; d < n; ++d) { r0->lo[d] = 0; r0->hi[d] = 1; }

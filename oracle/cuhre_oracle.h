@@ -53,6 +53,11 @@ typedef struct orc_integrand {
   int ndim;
   double a[ORC_MAXDIM];
   double u[ORC_MAXDIM];
+  /* integration box [box_lo, box_hi] when has_box, else the unit cube
+   * (the reference's Volume, GPUQuadVolume.cu:4-25, here in FP64) */
+  int has_box;
+  double box_lo[ORC_MAXDIM];
+  double box_hi[ORC_MAXDIM];
 } orc_integrand;
 
 typedef struct orc_rule orc_rule;
@@ -123,6 +128,8 @@ size_t orc_split(int ndim, size_t n, const double* lo, const double* len,
  * Writes d^ndim regions [ndim][count]; returns count.  If lo is NULL only
  * the count is returned. */
 size_t orc_initial_grid(int ndim, double* lo, double* len);
+/* The same grid laid over f's box (the unit cube when f has none). */
+size_t orc_initial_grid_box(const orc_integrand* f, double* lo, double* len);
 
 /* ---- phase 2 for one leftover box (GPUQuadPhases.cu:424-536), exact
  * max-error selection.  Returns the region count of the box. */

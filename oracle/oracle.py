@@ -36,6 +36,9 @@ class Integrand(C.Structure):
         ("ndim", C.c_int),
         ("a", C.c_double * MAXDIM),
         ("u", C.c_double * MAXDIM),
+        ("has_box", C.c_int),
+        ("box_lo", C.c_double * MAXDIM),
+        ("box_hi", C.c_double * MAXDIM),
     ]
 
 
@@ -123,7 +126,9 @@ def _ip(a: np.ndarray):
     return a.ctypes.data_as(C.POINTER(C.c_int))
 
 
-def make_integrand(family, ndim: int, a, u) -> Integrand:
+def make_integrand(family, ndim: int, a, u, lo=None, hi=None) -> Integrand:
+    """Integrand descriptor; lo/hi give an integration box (default the
+    unit cube)."""
     fam = FAMILY_NAMES[family] if isinstance(family, str) else int(family)
     f = Integrand()
     f.family = fam
@@ -133,6 +138,13 @@ def make_integrand(family, ndim: int, a, u) -> Integrand:
     for d in range(ndim):
         f.a[d] = float(a[d])
         f.u[d] = float(u[d])
+    if lo is not None or hi is not None:
+        blo = np.broadcast_to(np.asarray(0.0 if lo is None else lo, dtype=np.float64), (ndim,))
+        bhi = np.broadcast_to(np.asarray(1.0 if hi is None else hi, dtype=np.float64), (ndim,))
+        f.has_box = 1
+        for d in range(ndim):
+            f.box_lo[d] = float(blo[d])
+            f.box_hi[d] = float(bhi[d])
     return f
 
 

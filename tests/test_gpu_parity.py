@@ -378,3 +378,60 @@ def test_persistent_phase2_handoff(cub, ctx, count):
         assert p.status == m.status
         assert abs(p.integral - m.integral) <= 1e-3 * eps * abs(m.integral) + 1e-15
         assert abs(p.nregions - m.nregions) <= 0.01 * m.nregions + 4
+
+
+BOX_CASES = [
+    ("gaussian", 3, [3.0, 5.0, 4.0], [0.1, 0.9, 1.2], [-0.5, 0.25, 1.0], [0.75, 2.0, 1.5], 1e-8),
+    ("product_peak", 5, [8.0, 12.0, 6.0, 10.0, 9.0], [0.3, 1.6, -0.5, 0.4, 2.0],
+     [-1.0, 1.0, -2.0, 0.0, 1.5], [1.0, 2.5, 0.5, 0.5, 2.5], 1e-6),
+]
+
+
+@pytest.mark.parametrize("family,n,a,u,lo,hi,epsrel", BOX_CASES)
+def test_integrate_box_matches_oracle(cub, oracle, ctx, family, n, a, u, lo, hi, epsrel):
+    """Integration over a non-unit FP64 box (the reference's Volume) against
+    the oracle over the same box and the closed form."""
+    f_c = oracle.make_integrand(family, n, a, u, lo=lo, hi=hi)
+    r_c = oracle.Rule(n).integrate_reference(f_c, epsrel, 1e-14)
+    r_g = ctx.integrate(cub.Integrand(family, n, a, u), epsrel, 1e-14, lo=lo, hi=hi)
+    _compare_full(r_g, r_c, oracle.exact(f_c), epsrel, ("box", family, n))
+    q = cub.GPUcuhre(n).integrate(cub.Integrand(family, n, a, u), epsrel, 1e-14, vol=(lo, hi))
+    assert q.integral == r_g.integral and q.nregions == r_g.nregions
+
+
+def test_unit_box_is_the_default(cub, ctx):
+    """An explicit [0,1]^n box reproduces the unit-cube entry point bit for
+    bit (same grid arithmetic)."""
+    f = cub.Integrand("product_peak", 4, [8.0, 12.0, 6.0, 10.0], [0.3, 0.6, 0.5, 0.4])
+    r0 = ctx.integrate(f, 1e-6, 1e-12)
+    r1 = ctx.integrate(f, 1e-6, 1e-12, lo=0.0, hi=1.0)
+    assert (r1.integral, r1.error, r1.nregions, r1.status) == \
+        (r0.integral, r0.error, r0.nregions, r0.status)
+
+
+def test_batch_box_matches_single(cub, oracle, ctx):
+    rng = np.random.default_rng(17)
+    n, eps = 4, 1e-6
+    params, los, his, singles = [], [], [], []
+    for k in range(6):
+        a = np.exp(rng.uniform(0, np.log(20), n))
+        u = rng.uniform(-1, 2, n)
+        lo = rng.uniform(-1, 0.5, n)
+        hi = lo + rng.uniform(0.5, 2.0, n)
+        params.append(cub.make_params(n, list(a), list(u)))
+        los.append(list(lo))
+        his.append(list(hi))
+        singles.append(ctx.integrate(cub.Integrand("product_peak", n, list(a), list(u)), eps,
+                                     1e-14, lo=list(lo), hi=list(hi)))
+        ex = oracle.exact(oracle.make_integrand("product_peak", n, a, u, lo=lo, hi=hi))
+        assert abs(singles[-1].integral - ex) <= 2 * eps * ex
+    batch = ctx.integrate_batch("product_peak", n, params, eps, 1e-14, lo=los, hi=his)
+    for b, s in zip(batch, singles):
+        assert abs(b.integral - s.integral) <= 1e-13 * abs(s.integral)
+        assert b.nregions == s.nregions and b.status == s.status
+
+
+def test_box_rejects_empty_box(cub, ctx):
+    f = cub.Integrand("gaussian", 3, 4.0, 0.5)
+    with pytest.raises(cub.CubatureError):
+        ctx.integrate(f, 1e-6, 1e-12, lo=[0.0, 0.0, 1.0], hi=[1.0, 1.0, 1.0])

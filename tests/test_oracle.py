@@ -223,3 +223,30 @@ def test_reference_phase2_path(oracle):
     # neval bookkeeping of GPUKernelquad.cu:887-888
     full = R.integrate_reference(f, 1e-6, 1e-12)
     assert full["status"] == 0
+
+
+def test_unit_box_is_the_default(oracle):
+    """An explicit [0,1]^n box reproduces the default domain bit for bit."""
+    R = oracle.Rule(4)
+    a, u = [8.0, 12.0, 6.0, 10.0], [0.3, 0.6, 0.5, 0.4]
+    r0 = R.integrate_reference(oracle.make_integrand("product_peak", 4, a, u), 1e-6, 1e-12)
+    r1 = R.integrate_reference(oracle.make_integrand("product_peak", 4, a, u, lo=0.0, hi=1.0),
+                               1e-6, 1e-12)
+    assert r0 == r1
+
+
+@pytest.mark.parametrize("fam", ["gaussian", "product_peak"])
+def test_box_integration(oracle, fam):
+    """Integration over a non-unit box (the reference's Volume) against the
+    closed form over that box, by both CPU engines."""
+    lo, hi = [-0.5, 0.25, 1.0], [0.75, 2.0, 1.5]
+    f = oracle.make_integrand(fam, 3, [3.0, 5.0, 4.0], [0.1, 0.9, 1.2], lo=lo, hi=hi)
+    ex = oracle.exact(f)
+    assert math.isfinite(ex) and ex > 0
+    R = oracle.Rule(3)
+    r = R.integrate_reference(f, 1e-8, 1e-14)
+    assert r["status"] == 0
+    assert abs(r["value"] - ex) <= 1e-8 * ex
+    s = R.cuhre_sequential(f, 1e-8, 1e-14)
+    assert s["status"] == 0
+    assert abs(s["value"] - ex) <= 1e-8 * ex
