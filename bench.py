@@ -14,9 +14,12 @@ result).  Metric: integrals/s (whole job, all GPUs), with Geval/s beside it.
 oracle port of the two-phase engine, oracle/cuhre_oracle.c) on the host
 cores with all threads, on the same workload.
 
-Under torchrun each rank runs its own replica of the workload on its GPU
-(the path does not shard a single integral); steps are bracketed by a
-barrier and device synchronisation, and the max time over ranks is used.
+Under torchrun (weak scaling, no collective on the data path): for the
+single-integral workloads each rank integrates its own copy of the step's
+integrals; for batch workloads the job's world x count integrals are cut
+into contiguous shards, one per rank (cubature.parallel.shard_bounds).
+Steps are bracketed by a barrier and device synchronisation, and the max
+time over ranks is used.
 """
 from __future__ import annotations
 
@@ -300,16 +303,22 @@ def main() -> int:
         for f in items:
             exact.append(O.exact(O.make_integrand(f.family, f.ndim, f.a, f.u)))
     else:
+        # weak scaling: `count` integrals per rank; the job's world * count
+        # integrals (seed = global index) are cut into contiguous shards
+        from cubature.parallel import shard_bounds
+
         fam, n, count = workload["batch"]
-        plist = [cub.make_params(n, a, u) for a, u in product_peak_params(n, count)]
+        a0, b0 = shard_bounds(world * count, world, rank)
+        cases = product_peak_params(n, world * count)[a0:b0]
+        plist = [cub.make_params(n, a, u) for a, u in cases]
 
         def step():
             return ctx.integrate_batch(fam, n, plist, workload["epsrel"], workload["epsabs"], opts)
 
-        fams = [(fam, n)] * count
+        fams = [(fam, n)] * len(plist)
         import oracle as O
 
-        exact = [O.exact(O.make_integrand(fam, n, a, u)) for a, u in product_peak_params(n, count)]
+        exact = [O.exact(O.make_integrand(fam, n, a, u)) for a, u in cases]
 
     for _ in range(args.warmup):
         step()
@@ -355,6 +364,9 @@ def main() -> int:
         t = torch.tensor([dev_ms, wall], dtype=torch.float64, device="cuda")
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         dev_ms, wall = float(t[0]), float(t[1])
+        fb = torch.tensor([float(bad)], dtype=torch.float64, device="cuda")
+        pg.all_reduce(fb, op=pg.ReduceOp.SUM)
+        bad = int(fb[0])
     value = world * nint * args.steps / (dev_ms / 1e3)
     e2e_value = world * nint * args.steps / (wall / 1e3)
 
@@ -392,7 +404,8 @@ def main() -> int:
             "config": {"workload": args.workload, "integrals_per_step": nint,
                        "policy": workload.get("policy", "reference"),
                        "epsrel": workload["epsrel"], "epsabs": workload["epsabs"],
-                       "parallelism": "replicas" if world > 1 else "single",
+                       "parallelism": ("replicas" if "items" in workload else
+                                       f"shards{world}") if world > 1 else "single",
                        "l2": "flushed between steps (256 MB write)",
                        "regions_per_step": int(sum(nreg.values()))},
             "geval_per_s": world * neval * args.steps / (dev_ms / 1e3) / 1e9,

@@ -62,6 +62,7 @@ enum ErrorCode : int {
   kErrInvalid = -1,
   kErrCuda = -2,
   kErrCapacity = -3,
+  kErrUnsupported = -4,
   kErrTimeout = -5,
 };
 
@@ -106,10 +107,11 @@ class Workspace {
       if (p.first) cudaFree(p.first);
     bufs_.clear();
     bytes_ = 0;
-    if (ctl_host_) cudaFreeHost(ctl_host_);
+    if (host_block_) cudaFreeHost(host_block_);
+    host_block_ = nullptr;
     ctl_host_ = nullptr;
-    if (ist_host_) cudaFreeHost(ist_host_);
     ist_host_ = nullptr;
+    ctl_block_ = nullptr;
     for (auto& e : ev) {
       if (e) cudaEventDestroy(e);
       e = nullptr;
@@ -168,8 +170,13 @@ class Workspace {
   LeftoverResult* left_res = nullptr;
   IntegralState* ist = nullptr;
   Control* ctl = nullptr;
+  // The control block and the integral states share one device allocation
+  // (ctl, then ist at kStateOffset) and one pinned host copy (ctl_host_,
+  // ist_host_), so one copy moves both each way.
   Control* ctl_host_ = nullptr;
-  IntegralState* ist_host_ = nullptr;  // pinned staging of the integral states
+  IntegralState* ist_host_ = nullptr;
+  static constexpr size_t kStateOffset = (sizeof(Control) + 255) & ~size_t(255);
+  size_t state_bytes(int nint) const { return kStateOffset + sizeof(IntegralState) * nint; }
   void* slab = nullptr;
   int* heap = nullptr;
   int* counter = nullptr;
@@ -331,22 +338,25 @@ class Workspace {
       for (auto& e : ev)
         if (!ck(cudaEventCreate(&e))) return false;
     }
-    if (!ctl_host_) {
-      if (!ck(cudaMallocHost(&ctl_host_, sizeof(Control)))) return false;
-      if (!alloc(&ctl, sizeof(Control))) return false;
-      if (!alloc(&counter, sizeof(int) * 4)) return false;
-      if (!ck(cudaMemsetAsync(ctl, 0, sizeof(Control), s))) return false;
-    }
+    if (!counter && !alloc(&counter, sizeof(int) * 4)) return false;
     if (nint <= nint_cap_) return true;
-    free_buf(ist);
+    free_buf(ctl_block_);
+    ctl = nullptr;
+    ist = nullptr;
     free_buf(int_cnt);
-    if (ist_host_) cudaFreeHost(ist_host_);
+    if (host_block_) cudaFreeHost(host_block_);
+    host_block_ = nullptr;
+    ctl_host_ = nullptr;
     ist_host_ = nullptr;
     nint_cap_ = 0;
     const int n = std::max(nint, 64);
-    if (!alloc(&ist, sizeof(IntegralState) * n) || !alloc(&int_cnt, sizeof(unsigned) * n))
-      return false;
-    if (!ck(cudaMallocHost(&ist_host_, sizeof(IntegralState) * n))) return false;
+    if (!alloc(&ctl_block_, state_bytes(n)) || !alloc(&int_cnt, sizeof(unsigned) * n)) return false;
+    if (!ck(cudaMallocHost(&host_block_, state_bytes(n)))) return false;
+    ctl = static_cast<Control*>(ctl_block_);
+    ist = reinterpret_cast<IntegralState*>(static_cast<char*>(ctl_block_) + kStateOffset);
+    ctl_host_ = static_cast<Control*>(host_block_);
+    ist_host_ = reinterpret_cast<IntegralState*>(static_cast<char*>(host_block_) + kStateOffset);
+    if (!ck(cudaMemsetAsync(ctl, 0, sizeof(Control), s))) return false;
     if (!ck(cudaMemsetAsync(int_cnt, 0, sizeof(unsigned) * n, s))) return false;
     nint_cap_ = n;
     return true;
@@ -412,6 +422,8 @@ class Workspace {
   int nint_cap_ = 0;
   size_t slab_bytes_ = 0, heap_ints_ = 0;
   size_t box_cap_ = 0;
+  void* ctl_block_ = nullptr;
+  void* host_block_ = nullptr;
   size_t bytes_ = 0;
   std::string err_;
   Stats stats_;
@@ -484,16 +496,25 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
     is.seg_start = k * padded;
     is.seg_count = per;
   }
-  if (!ws.ck(cudaMemcpyAsync(ws.ist, h, sizeof(IntegralState) * nint, cudaMemcpyHostToDevice, s)))
-    return kErrCuda;
   Control c0;
   std::memset(&c0, 0, sizeof(c0));
   c0.host.n = (int)n_cur;
   c0.host.n_running = nint;
   *ws.ctl_host_ = c0;
-  if (!ws.ck(cudaMemcpyAsync(ws.ctl, ws.ctl_host_, sizeof(Control), cudaMemcpyHostToDevice, s)))
-    return kErrCuda;
-  st.h2d_bytes += (long long)(sizeof(IntegralState) * nint + sizeof(Control));
+  // The control block and the states go to the device with the first
+  // launch (one copy); the initial grid is written by k_init_grid or, when
+  // the persistent kernel runs first, by its first iteration.
+  bool uploaded = false;
+  bool grid_pending = true;
+  const double* d_box = nullptr;
+  if (h_box) {
+    const size_t nb = (size_t)nint * 2 * N;
+    if (!ws.reserve_boxes(nb)) return kErrCuda;
+    if (!ws.ck(cudaMemcpyAsync(ws.box, h_box, sizeof(double) * nb, cudaMemcpyHostToDevice, s)))
+      return kErrCuda;
+    st.h2d_bytes += (long long)(sizeof(double) * nb);
+    d_box = ws.box;
+  }
 
   int cur = 0;
   EngineArgs a;
@@ -529,21 +550,6 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
     a.left_cap = ws.left_cap();
   };
   bind(n_cur);
-  {
-    const long long blocks = std::min<long long>((n_cur + 255) / 256, (long long)sms * 8);
-    const double* d_box = nullptr;
-    if (h_box) {
-      const size_t nb = (size_t)nint * 2 * N;
-      if (!ws.reserve_boxes(nb)) return kErrCuda;
-      if (!ws.ck(cudaMemcpyAsync(ws.box, h_box, sizeof(double) * nb, cudaMemcpyHostToDevice, s)))
-        return kErrCuda;
-      st.h2d_bytes += (long long)(sizeof(double) * nb);
-      d_box = ws.box;
-    }
-    k_init_grid<N><<<(unsigned)std::max<long long>(blocks, 1), 256, 0, s>>>(a, dv, per, padded,
-                                                                          d_box);
-    st.launches += 1;
-  }
 
   // persistent kernel geometry (queried once per device and instantiation)
   int pblocks = 0;
@@ -565,7 +571,7 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
 
   IterState hs = c0.host;
   long long n_left = 0;
-  bool states_fresh = false;  // h holds the device states after the last kernel
+  bool states_fresh = true;  // h holds the device states after the last kernel
   int status = kOk;
   while (hs.n_running > 0 && hs.n > 0) {
     n_cur = hs.n;
@@ -593,9 +599,11 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
       ws.ctl_host_->timeout = 0;
       ws.ctl_host_->exit_reason = 0;
       std::memset(ws.ctl_host_->trace, 0, sizeof(ws.ctl_host_->trace));
-      if (!ws.ck(cudaMemcpyAsync(ws.ctl, ws.ctl_host_, sizeof(Control), cudaMemcpyHostToDevice, s)))
+      const size_t up = uploaded ? sizeof(Control) : ws.state_bytes(nint);
+      if (!ws.ck(cudaMemcpyAsync(ws.ctl, ws.ctl_host_, up, cudaMemcpyHostToDevice, s)))
         return kErrCuda;
-      st.h2d_bytes += sizeof(Control);
+      uploaded = true;
+      st.h2d_bytes += (long long)up;
       PersistArgs p;
       p.base = a;
       const long long nchunk = ws.cap() / 32 + 1;
@@ -613,6 +621,12 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
       p.iter_base = c0.iters_done;
       p.max_n = pmax;
       p.max_r = opt.persistent_max_r > 0 ? opt.persistent_max_r : 8;
+      p.init = grid_pending ? 1 : 0;
+      p.divisions = dv;
+      p.per_integral = per;
+      p.padded = padded;
+      p.box = d_box;
+      grid_pending = false;
       void* args[] = {(void*)&src, (void*)&T, (void*)&p};
       if (ws.timing) ws.ck(cudaEventRecord(ws.ev[0], s));
       if (!ws.ck(cudaLaunchCooperativeKernel((const void*)k_persistent<N, Src>, dim3(pblocks),
@@ -623,12 +637,11 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
       st.persistent_launches += 1;
       // the states come back with the control block: when the launch
       // finished every integral, no further round trip is needed
-      if (!ws.ck(cudaMemcpyAsync(ws.ctl_host_, ws.ctl, sizeof(Control), cudaMemcpyDeviceToHost, s)) ||
-          !ws.ck(cudaMemcpyAsync(h, ws.ist, sizeof(IntegralState) * nint, cudaMemcpyDeviceToHost,
-                                 s)))
+      if (!ws.ck(cudaMemcpyAsync(ws.ctl_host_, ws.ctl, ws.state_bytes(nint),
+                                 cudaMemcpyDeviceToHost, s)))
         return kErrCuda;
       if (!ws.ck(cudaStreamSynchronize(s))) return kErrCuda;
-      st.d2h_bytes += (long long)(sizeof(Control) + sizeof(IntegralState) * nint);
+      st.d2h_bytes += (long long)ws.state_bytes(nint);
       states_fresh = true;
       if (ws.timing) {
         float ms = 0;
@@ -652,6 +665,20 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
 
     // one iteration, one launch per step
     states_fresh = false;
+    if (!uploaded) {
+      if (!ws.ck(cudaMemcpyAsync(ws.ctl, ws.ctl_host_, ws.state_bytes(nint),
+                                 cudaMemcpyHostToDevice, s)))
+        return kErrCuda;
+      st.h2d_bytes += (long long)ws.state_bytes(nint);
+      uploaded = true;
+    }
+    if (grid_pending) {
+      const long long blocks = std::min<long long>((n_cur + 255) / 256, (long long)sms * 8);
+      k_init_grid<N><<<(unsigned)std::max<long long>(blocks, 1), 256, 0, s>>>(a, dv, per, padded,
+                                                                            d_box);
+      st.launches += 1;
+      grid_pending = false;
+    }
     int K = opt.lanes;
     if (K <= 0) K = n_cur >= (long long)sms * 512 ? 1 : (n_cur >= (long long)sms * 64 ? 8 : 32);
     if (ws.timing) ws.ck(cudaEventRecord(ws.ev[0], s));

@@ -517,31 +517,47 @@ static __global__ void k_advance(EngineArgs a) {
   }
 }
 
-// Initial grid for every integral: d^N equal boxes of its integration box
-// (box[k] = lo[N] then hi[N]; the unit cube when box is null),
-// GPUKernelquad.cu:24-61,300-316, dimension 0 varying fastest.
+// Slot t of the initial grid: integral t / padded, cell t % padded of the
+// d^N equal boxes of its integration box (box[k] = lo[N] then hi[N]; the
+// unit cube when box is null), dimension 0 varying fastest
+// (GPUKernelquad.cu:24-61,300-316).  Returns the integral, or -1 for a
+// padding slot.
+template <int N>
+__device__ __forceinline__ int initial_box(long long t, int divisions, int per_integral,
+                                           int padded, const double* box, double (&L)[N],
+                                           double (&H)[N]) {
+  const int k = (int)(t / padded);
+  const int j = (int)(t % padded);
+  if (j >= per_integral) return -1;
+  int rem = j;
+  const double* bx = box ? box + (long long)k * 2 * N : nullptr;
+#pragma unroll
+  for (int d = 0; d < N; ++d) {
+    const int id = rem % divisions;
+    rem /= divisions;
+    const double blo = bx ? bx[d] : 0.0;
+    const double w = (bx ? bx[N + d] - bx[d] : 1.0) / divisions;
+    L[d] = blo + id * w;
+    H[d] = w;
+  }
+  return k;
+}
+
+// Initial grid for every integral, written to the current list.
 template <int N>
 __global__ void k_init_grid(EngineArgs a, int divisions, int per_integral, int padded,
                             const double* box) {
   const long long total = (long long)a.nint * padded;
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
        t += (long long)gridDim.x * blockDim.x) {
-    const int k = (int)(t / padded);
-    const int j = (int)(t % padded);
-    if (j >= per_integral) {
-      const_cast<int*>(a.rid)[t] = -1;
-      continue;
-    }
-    int rem = j;
-    const double* bx = box ? box + (long long)k * 2 * N : nullptr;
+    double L[N], H[N];
+    const int k = initial_box<N>(t, divisions, per_integral, padded, box, L, H);
+    if (k >= 0) {
 #pragma unroll
-    for (int d = 0; d < N; ++d) {
-      const int id = rem % divisions;
-      rem /= divisions;
-      const double blo = bx ? bx[d] : 0.0;
-      const double w = (bx ? bx[N + d] - bx[d] : 1.0) / divisions;
-      const_cast<double*>(a.lo)[(long long)d * a.cap + t] = blo + id * w;
-      const_cast<double*>(a.len)[(long long)d * a.cap + t] = w;
+      for (int d = 0; d < N; ++d) {
+        const_cast<double*>(a.lo)[(long long)d * a.cap + t] = L[d];
+        const_cast<double*>(a.len)[(long long)d * a.cap + t] = H[d];
+      }
     }
     const_cast<int*>(a.rid)[t] = k;
   }

@@ -55,6 +55,18 @@ struct PersistArgs {
   int max_n;           // leave when the list is longer than this
   int max_r;           // most regions a block evaluates at once (1, 2, 4 or 8)
   int iter_base;       // global index of the launch's first iteration
+  // init != 0: the current list is the initial grid, not yet written; the
+  // first iteration computes each slot's box (initial_box) and writes it
+  int init;
+  int divisions, per_integral, padded;
+  const double* box;
+};
+
+// How the first step of an iteration obtains a slot's region.
+enum SlotSource : int {
+  kSlotStored = 0,  // read from the current list
+  kSlotLazy = 1,    // bisect the parent in the previous list
+  kSlotGrid = 2,    // compute the initial-grid box
 };
 
 namespace detail {
@@ -739,17 +751,37 @@ __device__ __forceinline__ Origin lazy_origin(const EngineArgs& a, const Stage& 
   return o;
 }
 
+// Write the initial grid in full (the kernel leaves before evaluating it).
+template <int N>
+__device__ void grid_pass(const PersistArgs& p, const Dest& D, long long n) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < n; s += stride) {
+    double L[N], H[N];
+    const int k = initial_box<N>(s, p.divisions, p.per_integral, p.padded, p.box, L, H);
+    if (k >= 0) {
+#pragma unroll
+      for (int d = 0; d < N; ++d) {
+        D.lo[(long long)d * D.cap + s] = L[d];
+        D.len[(long long)d * D.cap + s] = H[d];
+      }
+    }
+    D.rid[s] = k;
+  }
+}
+
 // The eval step with groups of G threads (R = 256/G regions per block).
 // The slots of round `base` are base + g * gridDim.x + blockIdx.x: group
 // index interleaved over blocks, so consecutive regions land on different
 // SMs.  Every group of a block runs the same number of rounds (groups past
-// the end of the list idle through the block barriers).  With `lazy`, the
-// group first bisects the slot's parent and writes the child into the list.
+// the end of the list idle through the block barriers).  Unless the slot's
+// region is stored, the group first computes it (lazy split or initial
+// grid) and writes it into the list.
 template <int N, int G, class Src>
 __device__ __forceinline__ void eval_step(const Src& src, const RuleTables& T, const EngineArgs& a,
-                                          const Parent& P, const Dest& D, const Stage& sg,
-                                          bool lazy, const IterState& st, IterState* next,
-                                          int* chunk_int, GroupSmem<N>& sm, int it, int g_next) {
+                                          const PersistArgs& pa, const Parent& P, const Dest& D,
+                                          const Stage& sg, int mode, const IterState& st,
+                                          IterState* next, int* chunk_int, GroupSmem<N>& sm,
+                                          int it, int g_next, const EngineArgs* sa) {
   constexpr int R = 256 / G;
   const int g = threadIdx.x / G, t = threadIdx.x % G, lane = threadIdx.x & 31;
   const long long ngroups = (long long)R * gridDim.x;
@@ -764,7 +796,23 @@ __device__ __forceinline__ void eval_step(const Src& src, const RuleTables& T, c
       L[d] = 0;
       H[d] = 1;
     }
-    if (live && !lazy) {
+    if (live && mode == kSlotGrid) {
+      k = initial_box<N>(slot, pa.divisions, pa.per_integral, pa.padded, pa.box, L, H);
+      if (k >= 0) {
+        epsrel = a.ist[k].epsrel;
+        epsabs = a.ist[k].epsabs;
+      }
+      if (t == 0) {
+        if (k >= 0) {
+#pragma unroll
+          for (int d = 0; d < N; ++d) {
+            D.lo[(long long)d * D.cap + slot] = L[d];
+            D.len[(long long)d * D.cap + slot] = H[d];
+          }
+        }
+        D.rid[slot] = k;
+      }
+    } else if (live && mode == kSlotStored) {
       k = a.rid[slot];
       if (k >= 0) {
 #pragma unroll
@@ -813,7 +861,7 @@ __device__ __forceinline__ void eval_step(const Src& src, const RuleTables& T, c
       // chunk's first slot always holds a region
       const long long c = slot / 32;
       const int kc = sm.owner[g] >= 0 ? sm.owner[g] : a.rid[c * 32];
-      after_chunk_warp(a, c, kc, lane, st, next, chunk_int, it, g_next);
+      after_chunk_warp(*sa, c, kc, lane, st, next, chunk_int, it, g_next);
     }
     __syncthreads();
   }
@@ -825,6 +873,7 @@ template <int N, class Src>
 __global__ void __launch_bounds__(256, 2) k_persistent(Src src, RuleTables T, PersistArgs p) {
   __shared__ detail::GroupSmem<N> sm;
   __shared__ detail::Stage sg;
+  __shared__ EngineArgs sargs;
   sm.pt.fill(threadIdx.x, blockDim.x);
   __syncthreads();
   Control* ctl = p.base.ctl;
@@ -847,6 +896,7 @@ __global__ void __launch_bounds__(256, 2) k_persistent(Src src, RuleTables T, Pe
       st.handoff = v->handoff;
     }
     const bool lazy = it > 0;
+    const int mode = lazy ? kSlotLazy : (p.init ? kSlotGrid : kSlotStored);
     EngineArgs a = p.base;
     a.lo = p.lo[cur];
     a.len = p.len[cur];
@@ -875,6 +925,8 @@ __global__ void __launch_bounds__(256, 2) k_persistent(Src src, RuleTables T, Pe
       if (lazy) {
         detail::materialize<N>(a, p.chunk_int, P, D);
         if (st.handoff) detail::handoff<N>(a, P, prid, prev_n, g_it);
+      } else if (mode == kSlotGrid) {
+        detail::grid_pass<N>(p, D, st.n);
       }
       break;
     }
@@ -902,22 +954,27 @@ __global__ void __launch_bounds__(256, 2) k_persistent(Src src, RuleTables T, Pe
       __syncthreads();
     }
     IterState* next = &ctl->it[parity ^ 1];
+    // The chain after a chunk runs out of line (one warp per chunk, cold
+    // code shared by all group sizes); it reads the arguments from a
+    // shared-memory copy so that the kernel's own copy stays in registers.
+    if (threadIdx.x == 0) sargs = a;
+    __syncthreads();
 
     // smallest R (regions per block) that covers the list in one pass
     const long long per_block = (st.n + gridDim.x - 1) / gridDim.x;
     const int r = per_block <= 1 ? 1 : (per_block <= 2 ? 2 : (per_block <= 4 ? 4 : 8));
     switch (r < p.max_r ? r : p.max_r) {
       case 1:
-        detail::eval_step<N, 256>(src, T, a, P, D, sg, lazy, st, next, p.chunk_int, sm, it, g_it + 1);
+        detail::eval_step<N, 256>(src, T, a, p, P, D, sg, mode, st, next, p.chunk_int, sm, it, g_it + 1, &sargs);
         break;
       case 2:
-        detail::eval_step<N, 128>(src, T, a, P, D, sg, lazy, st, next, p.chunk_int, sm, it, g_it + 1);
+        detail::eval_step<N, 128>(src, T, a, p, P, D, sg, mode, st, next, p.chunk_int, sm, it, g_it + 1, &sargs);
         break;
       case 4:
-        detail::eval_step<N, 64>(src, T, a, P, D, sg, lazy, st, next, p.chunk_int, sm, it, g_it + 1);
+        detail::eval_step<N, 64>(src, T, a, p, P, D, sg, mode, st, next, p.chunk_int, sm, it, g_it + 1, &sargs);
         break;
       default:
-        detail::eval_step<N, 32>(src, T, a, P, D, sg, lazy, st, next, p.chunk_int, sm, it, g_it + 1);
+        detail::eval_step<N, 32>(src, T, a, p, P, D, sg, mode, st, next, p.chunk_int, sm, it, g_it + 1, &sargs);
         break;
     }
     if (tracer) trace_mark(ctl, it, 4);

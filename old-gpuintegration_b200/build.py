@@ -59,6 +59,12 @@ def units() -> list[tuple[Path, Path, list[str]]]:
     return out
 
 
+# Example programs of the C++ front end (include/cubature/gpucuhre.cuh),
+# built as executables next to their sources; one dimension each.
+EXAMPLES = [(PKG / "examples" / "ref_api_example.cu", PKG / "examples" / "ref_api_example",
+             ["-DCUB_FRONT_MIN_DIM=3", "-DCUB_FRONT_MAX_DIM=3"])]
+
+
 def build(jobs: int | None = None, verbose: bool = False, extra: list[str] | None = None) -> Path:
     OBJ.mkdir(exist_ok=True)
     deps = _deps()
@@ -75,10 +81,24 @@ def build(jobs: int | None = None, verbose: bool = False, extra: list[str] | Non
             raise RuntimeError(f"nvcc failed for {obj.name}:\n{r.stderr[-4000:]}")
         return obj
 
-    if todo:
-        jobs = jobs or max(1, min(len(todo), os.cpu_count() or 1))
+    def link_example(item):
+        src, exe, defs = item
+        cmd = [cc, *NVCC_FLAGS, *(extra or []), *defs, str(src), "-o", str(exe), "-lcudart"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"nvcc failed for {exe.name}:\n{r.stderr[-4000:]}")
+        return exe
+
+    examples = [e for e in EXAMPLES if _stale(e[1], e[0], deps)]
+    if todo or examples:
+        jobs = jobs or max(1, min(len(todo) + len(examples), os.cpu_count() or 1))
         with ThreadPoolExecutor(jobs) as ex:
-            list(ex.map(compile_one, todo))
+            futs = [ex.submit(compile_one, t) for t in todo]
+            futs += [ex.submit(link_example, e) for e in examples]
+            for f in futs:
+                f.result()
     objs = [o for _, o, _ in units()]
     if todo or not LIB.exists() or any(o.stat().st_mtime > LIB.stat().st_mtime for o in objs):
         LIB.parent.mkdir(exist_ok=True)

@@ -1,0 +1,99 @@
+"""Independent integrals sharded across GPUs, one process per GPU.
+
+The reference distributes one integral's leftover regions over devices with
+MPI or OpenMP (GPUquad.h:430-609, GPUKernelquad.cu:729-906).  Here the unit
+of work is a whole integral: a batch of independent integrals is cut into
+contiguous shards, one per rank (torch.distributed, NCCL between GPUs or
+gloo on CPU), and each rank integrates its shard on its own device with no
+communication on the data path.  One gather of fixed-size result records at
+the end gives every rank the full result list.
+
+Failures are collective: a rank whose shard raises still joins the gather
+with an error mark, and every rank then raises, so no rank waits on a peer
+that has given up.
+"""
+from __future__ import annotations
+
+from typing import Callable, Sequence
+
+import torch
+import torch.distributed as dist
+
+from . import CubatureError, ERR_INVALID, Result
+
+_FIELDS = ("integral", "error", "nregions", "neval", "status", "iterations", "state")
+
+
+def shard_bounds(count: int, world: int, rank: int) -> tuple[int, int]:
+    """Contiguous shard [start, stop) of `count` items for `rank` of `world`;
+    shard sizes differ by at most one, the larger ones first."""
+    if world <= 0 or not 0 <= rank < world or count < 0:
+        raise ValueError("bad shard request")
+    base, extra = divmod(count, world)
+    start = rank * base + min(rank, extra)
+    return start, start + base + (1 if rank < extra else 0)
+
+
+def _pack(results: Sequence[Result], rows: int, failed: bool, device) -> torch.Tensor:
+    t = torch.zeros(rows, len(_FIELDS) + 2, dtype=torch.float64, device=device)
+    for i, r in enumerate(results):
+        t[i, : len(_FIELDS)] = torch.tensor([float(getattr(r, k)) for k in _FIELDS],
+                                            dtype=torch.float64)
+        t[i, -2] = 1.0  # row holds a result
+    t[:, -1] = 1.0 if failed else 0.0
+    return t
+
+
+def _unpack(row) -> Result:
+    v = [float(x) for x in row[: len(_FIELDS)]]
+    return Result(integral=v[0], error=v[1], nregions=int(v[2]), neval=int(v[3]),
+                  status=int(v[4]), iterations=int(v[5]), state=int(v[6]))
+
+
+def integrate_sharded(integrate: Callable[[int, int], Sequence[Result]], count: int,
+                      group=None) -> list[Result]:
+    """Run integrate(start, stop) on this rank's shard of `count` integrals
+    and return the results of all ranks, in order, on every rank.
+
+    `integrate` maps a shard to its results (for the GPU engine:
+    ``lambda a, b: ctx.integrate_batch(fam, n, params[a:b], ...)``).  Without
+    an initialised process group this is a plain call on the whole range."""
+    if not (dist.is_available() and dist.is_initialized()):
+        return list(integrate(0, count))
+    world = dist.get_world_size(group)
+    rank = dist.get_rank(group)
+    start, stop = shard_bounds(count, world, rank)
+    rows = max(1, shard_bounds(count, world, 0)[1])  # the largest shard
+    failed, message = False, ""
+    try:
+        local = list(integrate(start, stop)) if stop > start else []
+        if len(local) != stop - start:
+            raise CubatureError(ERR_INVALID, "shard returned the wrong number of results")
+    except Exception as exc:  # every rank must still reach the gather
+        failed, message, local = True, f"rank {rank}: {exc}", []
+    device = torch.device("cuda", torch.cuda.current_device()) \
+        if dist.get_backend(group) == "nccl" else torch.device("cpu")
+    mine = _pack(local, rows, failed, device)
+    parts = [torch.empty_like(mine) for _ in range(world)]
+    dist.all_gather(parts, mine, group=group)
+    bad = [r for r in range(world) if float(parts[r][0, -1]) != 0.0]
+    if bad:
+        raise CubatureError(ERR_INVALID, message or f"integration failed on rank(s) {bad}")
+    out: list[Result] = []
+    for r in range(world):
+        a, b = shard_bounds(count, world, r)
+        host = parts[r].cpu()
+        out.extend(_unpack(host[i]) for i in range(b - a))
+    return out
+
+
+def integrate_batch_sharded(ctx, family, ndim: int, params: Sequence, epsrel, epsabs,
+                            opts=None, group=None) -> list[Result]:
+    """ctx.integrate_batch over all ranks: each rank integrates its shard of
+    `params` on its own device (ctx is this rank's context)."""
+    def run(a: int, b: int):
+        er = epsrel if isinstance(epsrel, (int, float)) else list(epsrel)[a:b]
+        ea = epsabs if isinstance(epsabs, (int, float)) else list(epsabs)[a:b]
+        return ctx.integrate_batch(family, ndim, list(params)[a:b], er, ea, opts)
+
+    return integrate_sharded(run, len(params), group)

@@ -435,3 +435,32 @@ def test_box_rejects_empty_box(cub, ctx):
     f = cub.Integrand("gaussian", 3, 4.0, 0.5)
     with pytest.raises(cub.CubatureError):
         ctx.integrate(f, 1e-6, 1e-12, lo=[0.0, 0.0, 1.0], hi=[1.0, 1.0, 1.0])
+
+
+def test_reference_style_functor_front_end(oracle):
+    """A functor written the reference's way (double x[], int dim), compiled
+    against the C++ front end (quad::GPUcuhre, quad::Volume) as a caller of
+    the reference would: same answers as the oracle, unit cube and box."""
+    import json
+    import subprocess
+    from pathlib import Path
+
+    exe = Path(__file__).resolve().parents[1] / "old-gpuintegration_b200" / "examples" / \
+        "ref_api_example"
+    assert exe.exists(), "build the examples with old-gpuintegration_b200/build.py"
+    eps, lo, hi = 1e-7, -0.5, 1.5
+    out = subprocess.run([str(exe), repr(eps), repr(lo), repr(hi)], capture_output=True,
+                         text=True, timeout=120, check=True).stdout
+    rows = [json.loads(line) for line in out.splitlines() if line.startswith("{")]
+    assert [r["box"] for r in rows] == [False, True]
+    a, u = [8.0, 12.0, 6.0], [0.3, 0.6, 0.5]
+    for r in rows:
+        box = dict(lo=lo, hi=hi) if r["box"] else {}
+        f_c = oracle.make_integrand("product_peak", 3, a, u, **box)
+        r_c = oracle.Rule(3).integrate_reference(f_c, eps, 1e-14)
+        assert r["flag"] == r_c["status"] == 0
+        assert abs(r["integral"] - r_c["value"]) <= 2 * eps * abs(r_c["value"])
+        assert abs(r["integral"] - oracle.exact(f_c)) <= 2 * eps * oracle.exact(f_c)
+        assert abs(r["nregions"] - r_c["nregions"]) <= 0.02 * r_c["nregions"] + 4
+        if r_c["phase2_regions"] == 0:
+            assert r["neval"] == r["nregions"] * oracle.Rule(3).npoints

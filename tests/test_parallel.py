@@ -1,0 +1,122 @@
+"""Sharding independent integrals across ranks (cubature.parallel), run as
+two gloo processes on CPU.  Each rank integrates its shard with the oracle's
+two-phase engine (the per-rank integrator is a parameter), so the sharding,
+gathering and failure paths are checked without a GPU."""
+import os
+import socket
+import sys
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+sys.path.insert(0, str(ROOT / "old-gpuintegration_b200"))
+sys.path.insert(0, str(ROOT / "oracle"))
+
+torch = pytest.importorskip("torch")
+import torch.distributed as dist  # noqa: E402
+import torch.multiprocessing as mp  # noqa: E402
+
+from cubature import parallel as P  # noqa: E402
+
+
+def test_shard_bounds_cover_exactly():
+    for count in [0, 1, 5, 7, 64, 4096, 4097]:
+        for world in [1, 2, 3, 8]:
+            got = [P.shard_bounds(count, world, r) for r in range(world)]
+            assert got[0][0] == 0 and got[-1][1] == count
+            assert all(a[1] == b[0] for a, b in zip(got, got[1:]))
+            sizes = [b - a for a, b in got]
+            assert max(sizes) - min(sizes) <= 1 and sizes == sorted(sizes, reverse=True)
+    with pytest.raises(ValueError):
+        P.shard_bounds(4, 2, 2)
+
+
+def test_without_process_group_runs_whole_range():
+    calls = []
+    out = P.integrate_sharded(lambda a, b: calls.append((a, b)) or
+                              [P.Result(1.0, 0.0, 1, 1, 0, 1, 1)] * (b - a), 3)
+    assert calls == [(0, 3)] and len(out) == 3
+
+
+def _cases(count):
+    import numpy as np
+
+    rng = np.random.default_rng(11)
+    return [(list(np.exp(rng.uniform(0, np.log(20), 3))), list(rng.uniform(0.1, 0.9, 3)))
+            for _ in range(count)]
+
+
+def _oracle_shard(cases, a, b):
+    import oracle as O
+
+    R = O.Rule(3)
+    out = []
+    for av, uv in cases[a:b]:
+        r = R.integrate_reference(O.make_integrand("product_peak", 3, av, uv), 1e-6, 1e-12)
+        out.append(P.Result(r["value"], r["error"], r["nregions"], r["neval"], r["status"],
+                            r["phase1_iters"], 1))
+    return out
+
+
+def _worker(rank, world, port, count, fail_rank, q):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    from datetime import timedelta
+
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+    try:
+        cases = _cases(count)
+
+        def shard(a, b):
+            if rank == fail_rank:
+                raise RuntimeError("injected failure")
+            return _oracle_shard(cases, a, b)
+
+        try:
+            res = P.integrate_sharded(shard, count)
+            q.put((rank, "ok", [(r.integral, r.nregions, r.status) for r in res]))
+        except P.CubatureError as exc:
+            q.put((rank, "error", str(exc)))
+    finally:
+        dist.destroy_process_group()
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _run(world, count, fail_rank=-1):
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, world, port, count, fail_rank, q))
+             for r in range(world)]
+    for p in procs:
+        p.start()
+    out = [q.get(timeout=120) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    return sorted(out)
+
+
+@pytest.mark.parametrize("count", [5, 8])
+def test_sharded_matches_serial(count):
+    """Two ranks, each integrating its shard: every rank gets the full
+    result list, identical to integrating the batch in one process."""
+    serial = [(r.integral, r.nregions, r.status) for r in _oracle_shard(_cases(count), 0, count)]
+    out = _run(2, count)
+    assert [o[1] for o in out] == ["ok", "ok"]
+    for _, _, res in out:
+        assert res == serial
+
+
+def test_failure_on_one_rank_reaches_all():
+    """A shard that raises on rank 1 makes both ranks raise (no rank is left
+    waiting in the gather)."""
+    out = _run(2, 6, fail_rank=1)
+    assert [o[1] for o in out] == ["error", "error"]
+    assert all("rank 1" in o[2] or "rank(s) [1]" in o[2] for o in out)
