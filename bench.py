@@ -156,6 +156,19 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def profiled_traffic(kernel: str, workload: str):
+    """DRAM bytes (read + write) per launch of `kernel` on `workload` from
+    the committed ncu summary profiles/<kernel>_<workload>.md (the line
+    'traffic_bytes_per_launch: N'); None when there is no such capture."""
+    import re
+
+    path = ROOT / "profiles" / f"{kernel}_{workload}.md"
+    if not path.exists():
+        return None
+    m = re.search(r"^traffic_bytes_per_launch:\s*(\d+)", path.read_text(), re.M)
+    return int(m.group(1)) if m else None
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -413,11 +426,11 @@ def main() -> int:
                     "h2d_bytes_per_step": st.get("h2d_bytes", 0) // max(1, args.steps),
                     "d2h_bytes_per_step": st.get("d2h_bytes", 0) // max(1, args.steps)},
             "gpu_launches": st["launches"],
-            "roofline": {"kernel": dom, "bound": "fp64", "achieved": achieved,
+            "roofline": {"kernel": dom, "bound": "tensor", "pipe": "fp64", "achieved": achieved,
                          "peak": peak, "unit": "TFLOP/s",
                          "frac": (achieved / peak) if achieved and peak else None,
-                         "traffic": None,
-                         "peak_source": "in-run cuBLAS DGEMM 8192^3 (MEASURED_PEAKS.json has no FP64 figure)",
+                         "traffic": profiled_traffic(dom, args.workload),
+                         "peak_source": "in-run cuBLAS DGEMM 8192^3 on the FP64 tensor pipe (MEASURED_PEAKS.json has no FP64 figure)",
                          "algorithmic_flops_per_region": mean_flops,
                          "kernel_ms_per_step": {k: v[1] / args.steps for k, v in kernels.items()},
                          "regions_per_step": {"k_persistent": pk_regions / args.steps,
