@@ -198,6 +198,60 @@ int cub_integrate_batch_box(cub_ctx* ctx, int family, int ndim, int count,
                             const double* epsrel, const double* epsabs, double epsrel0,
                             double epsabs0, const cub_options* opt, cub_result* out);
 
+/* ---- integrands on device tables ------------------------------------- */
+
+/* Rectilinear 2-D table in device memory, row-major zs[i * ny + j] at
+ * (xs[i], ys[j]), knots ascending, nx, ny >= 2: the reference's Interp2D
+ * (GPUQuadInterp2D.cu:50-106), evaluated in FP64 with a binary search for
+ * the cell (the reference reads FP32 textures and searches linearly).
+ * Points outside the knots extrapolate linearly from the end cells. */
+typedef struct cub_interp2d {
+  const double* xs;
+  const double* ys;
+  const double* zs;
+  int nx, ny;
+} cub_interp2d;
+
+/* Natural cubic spline in device memory: knots xs (ascending), values ys,
+ * second derivatives y2 (cub_spline_second_derivatives), n >= 2. */
+typedef struct cub_spline1d {
+  const double* xs;
+  const double* ys;
+  const double* y2;
+  int n;
+} cub_spline1d;
+
+/* The five tables of the LC_LT integrand (tau, mu, sigma, fmsk, fprj) over
+ * (lt, zt); all five share xs, ys, nx, ny of the first. */
+typedef struct cub_lclt_tables {
+  cub_interp2d t[5];
+} cub_lclt_tables;
+
+/* The 7-D table integrand: spline(x0) * bilinear(x1, x2) *
+ * exp(-(4 x3 - mu)^2 / (2 sigma^2)), mu = offset + 2 x4 + 0.1 (x5 + x6). */
+typedef struct cub_table7 {
+  cub_spline1d spline;
+  cub_interp2d grid;
+  double sigma;
+} cub_table7;
+
+/* Natural cubic spline second derivatives for n knots (host memory). */
+int cub_spline_second_derivatives(int n, const double* xs, const double* ys, double* y2);
+
+/* The reference's LC_LT integrand (lc_lt_t.h:18-52) over the box [lo, hi]
+ * in (lt, zt, lc), in FP64; tables in device memory, owned by the caller. */
+int cub_integrate_lclt(cub_ctx* ctx, const cub_lclt_tables* tables, const double* lo,
+                       const double* hi, double epsrel, double epsabs, const cub_options* opt,
+                       cub_result* out);
+
+/* `count` integrals of the 7-D table integrand over [0,1]^7, one mu offset
+ * each (host array), on one shared region list.  epsrel/epsabs as in
+ * cub_integrate_batch. */
+int cub_integrate_table7_batch(cub_ctx* ctx, const cub_table7* tables, int count,
+                               const double* offsets, const double* epsrel, const double* epsabs,
+                               double epsrel0, double epsabs0, const cub_options* opt,
+                               cub_result* out);
+
 /* ---- per-step entry points on caller device buffers ------------------ */
 
 /* Rule tables of the degree-9 rule for ndim (GPUQuadRule.cu:31-228):

@@ -16,6 +16,41 @@ thread_local std::string g_error;
 
 void set_error(const std::string& msg) { g_error = msg; }
 
+int cuda_error(cudaError_t e, const char* what) {
+  set_error(std::string(what) + ": " + cudaGetErrorString(e));
+  return CUB_ERR_CUDA;
+}
+
+int engine_status(cub_ctx* ctx, int rc) {
+  switch (rc) {
+    case kOk:
+      return 0;
+    case kErrCuda:
+      set_error(ctx->ws->error());
+      return CUB_ERR_CUDA;
+    case kErrTimeout:
+      set_error("a device-side grid barrier wait ran out (persistent kernel)");
+      return CUB_ERR_TIMEOUT;
+    case kErrCapacity:
+      set_error("region capacity exceeded; results are the last estimates");
+      return CUB_ERR_CAPACITY;
+    default:
+      set_error("invalid argument");
+      return rc < 0 ? rc : CUB_ERR_INVALID;
+  }
+}
+
+void result_to_c(const Result& r, cub_result* c) {
+  c->value = r.value;
+  c->error = r.error;
+  c->nregions = r.nregions;
+  c->neval = r.neval;
+  c->status = r.status;
+  c->iterations = r.iterations;
+  c->state = r.state;
+  c->reserved = 0;
+}
+
 cudaStream_t as_stream(void* s) { return static_cast<cudaStream_t>(s); }
 
 Options to_options(const cub_options* opt) {
@@ -143,6 +178,7 @@ void cub_destroy(cub_ctx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   delete ctx->ws;
   if (ctx->d_params) cudaFree(ctx->d_params);
+  if (ctx->d_aux) cudaFree(ctx->d_aux);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
 }
@@ -190,6 +226,9 @@ void cub_ctx_release(cub_ctx* ctx) {
   if (ctx->d_params) cudaFree(ctx->d_params);
   ctx->d_params = nullptr;
   ctx->params_cap = 0;
+  if (ctx->d_aux) cudaFree(ctx->d_aux);
+  ctx->d_aux = nullptr;
+  ctx->aux_cap = 0;
 }
 
 void cub_ctx_reset_stats(cub_ctx* ctx) {

@@ -14,12 +14,18 @@ struct cub_ctx {
   cubature::Workspace* ws = nullptr;
   cubature::GenzParams* d_params = nullptr;
   int params_cap = 0;
+  double* d_aux = nullptr;  // per-integral scalars of the table integrands
+  int aux_cap = 0;
 };
 
 namespace cubature {
 namespace capi {
 
 void set_error(const std::string& msg);
+int cuda_error(cudaError_t e, const char* what);
+// Map an engine return code to the C ABI (sets the message).
+int engine_status(cub_ctx* ctx, int rc);
+void result_to_c(const Result& r, cub_result* c);
 cudaStream_t as_stream(void* s);
 Options to_options(const cub_options* opt);
 

@@ -108,7 +108,8 @@ EXPORTS = (
     "cub_split_scratch_bytes", "cub_reduce_scratch_bytes", "cub_split", "cub_reduce",
     "cub_ctx_stream", "cub_ctx_stats", "cub_ctx_reset_stats", "cub_ctx_set_timing",
     "cub_ctx_release", "cub_split_noalloc", "cub_ctx_trace", "cub_integrate_box",
-    "cub_integrate_batch_box",
+    "cub_integrate_batch_box", "cub_spline_second_derivatives", "cub_integrate_lclt",
+    "cub_integrate_table7_batch",
 )
 
 _lib = None
@@ -143,6 +144,11 @@ def load_library(path: str | Path | None = None):
     L.cub_integrate_batch_box.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.POINTER(GenzParams),
                                           dp, dp, dp, dp, C.c_double, C.c_double,
                                           C.POINTER(COptions), C.POINTER(CResult)]
+    L.cub_spline_second_derivatives.argtypes = [C.c_int, dp, dp, dp]
+    L.cub_integrate_lclt.argtypes = [vp, vp, dp, dp, C.c_double, C.c_double, C.POINTER(COptions),
+                                     C.POINTER(CResult)]
+    L.cub_integrate_table7_batch.argtypes = [vp, vp, C.c_int, dp, dp, dp, C.c_double, C.c_double,
+                                             C.POINTER(COptions), C.POINTER(CResult)]
     L.cub_ctx_stream.argtypes = [vp]
     L.cub_ctx_stream.restype = vp
     L.cub_ctx_stats.argtypes = [vp, C.POINTER(CStats)]
@@ -370,6 +376,54 @@ class Context:
         if rc < 0 and rc != ERR_CAPACITY:
             raise CubatureError(rc, last_error())
         return [Result.from_c(out[i]) for i in range(n)]
+
+
+    def integrate_lclt(self, tables, lo, hi, epsrel: float, epsabs: float,
+                       opts: COptions | None = None) -> Result:
+        """The reference's LC_LT integrand over the box [lo, hi] in (lt, zt,
+        lc); `tables` is a cubature.tables.LcLtTables."""
+        out = CResult()
+        blo = (C.c_double * 3)(*_axis_values(lo, 3))
+        bhi = (C.c_double * 3)(*_axis_values(hi, 3))
+        _check(self._lib.cub_integrate_lclt(self._h, C.byref(tables.c), blo, bhi, epsrel, epsabs,
+                                            C.byref(opts) if opts else None, C.byref(out)))
+        return Result.from_c(out)
+
+    def integrate_table7_batch(self, tables, offsets, epsrel, epsabs,
+                               opts: COptions | None = None) -> list[Result]:
+        """The 7-D table integrand for each mu offset; `tables` is a
+        cubature.tables.Table7."""
+        n = len(offsets)
+        off = (C.c_double * n)(*[float(x) for x in offsets])
+        out = (CResult * n)()
+        er = ea = None
+        er0 = ea0 = 0.0
+        if isinstance(epsrel, (int, float)):
+            er0 = float(epsrel)
+        else:
+            er = (C.c_double * n)(*[float(x) for x in epsrel])
+        if isinstance(epsabs, (int, float)):
+            ea0 = float(epsabs)
+        else:
+            ea = (C.c_double * n)(*[float(x) for x in epsabs])
+        rc = self._lib.cub_integrate_table7_batch(self._h, C.byref(tables.c), n, off, er, ea, er0,
+                                                  ea0, C.byref(opts) if opts else None, out)
+        if rc < 0 and rc != ERR_CAPACITY:
+            raise CubatureError(rc, last_error())
+        return [Result.from_c(out[i]) for i in range(n)]
+
+def spline_second_derivatives(xs, ys):
+    """Natural cubic spline second derivatives (host), for device splines."""
+    import numpy as np
+
+    xs = np.ascontiguousarray(xs, dtype=np.float64)
+    ys = np.ascontiguousarray(ys, dtype=np.float64)
+    y2 = np.zeros_like(xs)
+    dp = C.POINTER(C.c_double)
+    _check(load_library().cub_spline_second_derivatives(len(xs), xs.ctypes.data_as(dp),
+                                                        ys.ctypes.data_as(dp),
+                                                        y2.ctypes.data_as(dp)))
+    return y2
 
 
 def _axis_values(v, ndim: int) -> list[float]:

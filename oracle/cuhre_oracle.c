@@ -242,10 +242,94 @@ void orc_rule_points(const orc_rule* r, double* g, int* set)
  * Integrand families (Genz 1984 test families; COSSUM is the reference's
  * own driver integrand, cudaCuhre.cu:11-22).
  * ---------------------------------------------------------------------- */
+/* ------------------------------------------------------------------------
+ * Tables: cell search (the cell left of the first knot >= t among
+ * xs[1..n-1], as the reference's SmallNearestN, GPUQuadInterp2D.cu:50-67,
+ * clamped to the table), bilinear interpolation, natural cubic spline.
+ * ---------------------------------------------------------------------- */
+int orc_table_cell(const double* xs, int n, double t)
+{
+  int i = 1;
+  while (i < n - 1 && xs[i] < t) ++i;
+  return i - 1;
+}
+
+double orc_interp2d_eval(const orc_interp2d* t, double x, double y)
+{
+  const int i = orc_table_cell(t->xs, t->nx, x), j = orc_table_cell(t->ys, t->ny, y);
+  const double x1 = t->xs[i], x2 = t->xs[i + 1], y1 = t->ys[j], y2 = t->ys[j + 1];
+  const double q11 = t->zs[i * t->ny + j], q21 = t->zs[(i + 1) * t->ny + j];
+  const double q12 = t->zs[i * t->ny + j + 1], q22 = t->zs[(i + 1) * t->ny + j + 1];
+  const double d = (x2 - x1) * (y2 - y1);
+  return (q11 * (x2 - x) + q21 * (x - x1)) * ((y2 - y) / d) +
+         (q12 * (x2 - x) + q22 * (x - x1)) * ((y - y1) / d);
+}
+
+double orc_spline_eval(const orc_spline1d* s, double t)
+{
+  const int i = orc_table_cell(s->xs, s->n, t);
+  const double h = s->xs[i + 1] - s->xs[i];
+  const double a = (s->xs[i + 1] - t) / h, b = (t - s->xs[i]) / h;
+  return a * s->ys[i] + b * s->ys[i + 1] +
+         ((a * a * a - a) * s->y2[i] + (b * b * b - b) * s->y2[i + 1]) * (h * h) / 6.0;
+}
+
+void orc_spline_second_derivs(int n, const double* xs, const double* ys, double* y2)
+{
+  /* natural end conditions; Thomas algorithm on the interior equations
+   * h_{i-1} y2_{i-1} + 2 (h_{i-1} + h_i) y2_i + h_i y2_{i+1} = 6 (d_i - d_{i-1}) */
+  double* c = (double*)malloc(sizeof(double) * (size_t)n);
+  double* r = (double*)malloc(sizeof(double) * (size_t)n);
+  y2[0] = 0;
+  y2[n - 1] = 0;
+  c[0] = 0;
+  r[0] = 0;
+  for (int i = 1; i < n - 1; ++i) {
+    const double hl = xs[i] - xs[i - 1], hr = xs[i + 1] - xs[i];
+    const double rhs = 6.0 * ((ys[i + 1] - ys[i]) / hr - (ys[i] - ys[i - 1]) / hl);
+    const double den = 2.0 * (hl + hr) - hl * c[i - 1];
+    c[i] = hr / den;
+    r[i] = (rhs - hl * r[i - 1]) / den;
+  }
+  for (int i = n - 2; i >= 1; --i) y2[i] = r[i] - c[i] * y2[i + 1];
+  free(c);
+  free(r);
+}
+
+static double lclt_eval(const orc_tables* T, const double* x)
+{
+  const double lt = x[0], zt = x[1], lc = x[2];
+  double v[5];
+  for (int q = 0; q < 5; ++q) v[q] = orc_interp2d_eval(&T->lclt[q], lt, zt);
+  const double tau = v[0], mu = v[1], sigma = v[2], fmsk = v[3], fprj = v[4];
+  /* lc_lt_t.h:36-50 */
+  const double exptau = exp(tau * (2.0 * mu + tau * sigma * sigma - 2.0 * lc) / 2.0);
+  const double r2s = sqrt(2.0) * sigma;
+  const double mts = mu + tau * sigma * sigma;
+  const double zg = (lc - mu) / sigma;
+  const double gauss = exp(-zg * zg / 2.0) * 0.3989422804014327 / sigma;
+  return (1.0 - fmsk) * (1.0 - fprj) * gauss +
+         0.5 * ((1.0 - fmsk) * fprj * tau + fmsk * fprj / lt) * exptau * erfc((mts - lc) / r2s) +
+         0.5 * fmsk / lt * (erfc((lc - mu) / r2s) - erfc((lc + lt - mu) / r2s)) -
+         0.5 * fmsk * fprj / lt * (exp(-tau * lt) * exptau * erfc((mts - lc - lt) / r2s));
+}
+
+static double table7_eval(const orc_tables* T, const double* x)
+{
+  const double mu = T->offset + 2.0 * x[4] + 0.1 * (x[5] + x[6]);
+  const double r = 4.0 * x[3] - mu;
+  return orc_spline_eval(&T->spline, x[0]) * orc_interp2d_eval(&T->grid, x[1], x[2]) *
+         exp(-r * r / (2.0 * T->sigma * T->sigma));
+}
+
 double orc_eval_integrand(const orc_integrand* f, const double* x)
 {
   const int n = f->ndim;
   switch (f->family) {
+    case ORC_LCLT:
+      return lclt_eval(f->tables, x);
+    case ORC_TABLE7:
+      return table7_eval(f->tables, x);
     case ORC_GAUSSIAN: {
       double s = 0;
       for (int d = 0; d < n; ++d) {

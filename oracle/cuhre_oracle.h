@@ -37,9 +37,40 @@ enum {
   ORC_PRODUCT_PEAK = 4,  /* prod 1/(a_i^-2 + (x_i-u_i)^2)                  */
   ORC_CONTINUOUS = 5,    /* exp(-sum a_i |x_i-u_i|)                        */
   ORC_DISCONTINUOUS = 6, /* 0 if x_0>u_0 or x_1>u_1 else exp(sum a_i x_i)  */
-  ORC_COSSUM = 7         /* -sum cos(10 x_i)/0.054402111088937 / 2
+  ORC_COSSUM = 7,        /* -sum cos(10 x_i)/0.054402111088937 / 2
                             (cudaCuhre.cu:11-22, function.cu:111-117)      */
+  ORC_LCLT = 8,          /* LC_LT over (lt, zt, lc) from five 2-D tables
+                            (lc_lt_t.h:18-52)                              */
+  ORC_TABLE7 = 9         /* spline(x0) bilinear(x1,x2)
+                            exp(-(4 x3 - mu)^2 / 2 sigma^2),
+                            mu = offset + 2 x4 + 0.1 (x5 + x6)            */
 };
+
+/* Rectilinear 2-D table, row-major zs[i * ny + j] at (xs[i], ys[j]); the
+ * reference's Interp2D (GPUQuadInterp2D.cu:50-106) in FP64. */
+typedef struct orc_interp2d {
+  const double* xs;
+  const double* ys;
+  const double* zs;
+  int nx, ny;
+} orc_interp2d;
+
+/* Natural cubic spline: knots, values, second derivatives. */
+typedef struct orc_spline1d {
+  const double* xs;
+  const double* ys;
+  const double* y2;
+  int n;
+} orc_spline1d;
+
+/* Tables of the table integrands (host memory, owned by the caller). */
+typedef struct orc_tables {
+  orc_interp2d lclt[5];  /* tau, mu, sigma, fmsk, fprj on one grid         */
+  orc_spline1d spline;   /* TABLE7 */
+  orc_interp2d grid;     /* TABLE7 */
+  double sigma;          /* TABLE7 kernel width */
+  double offset;         /* TABLE7 mu offset */
+} orc_tables;
 
 /* Policy for classifying regions as finished. */
 enum {
@@ -58,6 +89,7 @@ typedef struct orc_integrand {
   int has_box;
   double box_lo[ORC_MAXDIM];
   double box_hi[ORC_MAXDIM];
+  const orc_tables* tables;  /* ORC_LCLT, ORC_TABLE7 */
 } orc_integrand;
 
 typedef struct orc_rule orc_rule;
@@ -82,6 +114,13 @@ typedef struct orc_out {
   size_t phase2_regions; /* leftover regions handed to phase 2            */
   size_t phase2_failed;
 } orc_out;
+
+/* ---- tables ---- */
+int orc_table_cell(const double* xs, int n, double t);
+double orc_interp2d_eval(const orc_interp2d* t, double x, double y);
+double orc_spline_eval(const orc_spline1d* s, double t);
+/* Natural cubic spline second derivatives (tridiagonal solve). */
+void orc_spline_second_derivs(int n, const double* xs, const double* ys, double* y2);
 
 /* ---- rule (GPUQuadRule.cu:31-390) ---- */
 orc_rule* orc_rule_new(int ndim);

@@ -39,7 +39,23 @@ class Integrand(C.Structure):
         ("has_box", C.c_int),
         ("box_lo", C.c_double * MAXDIM),
         ("box_hi", C.c_double * MAXDIM),
+        ("tables", C.c_void_p),
     ]
+
+
+class Interp2DC(C.Structure):
+    _fields_ = [("xs", C.POINTER(C.c_double)), ("ys", C.POINTER(C.c_double)),
+                ("zs", C.POINTER(C.c_double)), ("nx", C.c_int), ("ny", C.c_int)]
+
+
+class Spline1DC(C.Structure):
+    _fields_ = [("xs", C.POINTER(C.c_double)), ("ys", C.POINTER(C.c_double)),
+                ("y2", C.POINTER(C.c_double)), ("n", C.c_int)]
+
+
+class TablesC(C.Structure):
+    _fields_ = [("lclt", Interp2DC * 5), ("spline", Spline1DC), ("grid", Interp2DC),
+                ("sigma", C.c_double), ("offset", C.c_double)]
 
 
 class Result(C.Structure):
@@ -114,6 +130,13 @@ def lib():
         L.orc_cuhre_sequential.argtypes = [C.c_void_p, C.POINTER(Integrand), C.c_double,
                                            C.c_double, C.c_size_t, C.POINTER(Out)]
         L.orc_max_threads.restype = C.c_int
+        L.orc_table_cell.argtypes = [dp, C.c_int, C.c_double]
+        L.orc_table_cell.restype = C.c_int
+        L.orc_interp2d_eval.argtypes = [C.POINTER(Interp2DC), C.c_double, C.c_double]
+        L.orc_interp2d_eval.restype = C.c_double
+        L.orc_spline_eval.argtypes = [C.POINTER(Spline1DC), C.c_double]
+        L.orc_spline_eval.restype = C.c_double
+        L.orc_spline_second_derivs.argtypes = [C.c_int, dp, dp, dp]
         _lib = L
     return _lib
 
@@ -277,3 +300,74 @@ def max_threads() -> int:
 
 
 os.environ.setdefault("OMP_PROC_BIND", "false")
+
+
+# -- table integrands ------------------------------------------------------
+LCLT, TABLE7 = 8, 9
+FAMILY_NAMES["lclt"] = LCLT
+FAMILY_NAMES["table7"] = TABLE7
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def interp2d(xs, ys, zs):
+    """Host table for the oracle (keeps its arrays alive on the struct)."""
+    xs, ys, zs = _f64(xs), _f64(ys), _f64(zs).reshape(len(xs), len(ys))
+    t = Interp2DC(_dp(xs), _dp(ys), _dp(zs), len(xs), len(ys))
+    t._keep = (xs, ys, zs)
+    return t
+
+
+def spline_second_derivs(xs, ys) -> np.ndarray:
+    xs, ys = _f64(xs), _f64(ys)
+    y2 = np.zeros_like(xs)
+    lib().orc_spline_second_derivs(len(xs), _dp(xs), _dp(ys), _dp(y2))
+    return y2
+
+
+def spline1d(xs, ys, y2=None):
+    xs, ys = _f64(xs), _f64(ys)
+    y2 = spline_second_derivs(xs, ys) if y2 is None else _f64(y2)
+    s = Spline1DC(_dp(xs), _dp(ys), _dp(y2), len(xs))
+    s._keep = (xs, ys, y2)
+    return s
+
+
+def interp2d_eval(t: Interp2DC, x: float, y: float) -> float:
+    return lib().orc_interp2d_eval(C.byref(t), x, y)
+
+
+def spline_eval(s: Spline1DC, t: float) -> float:
+    return lib().orc_spline_eval(C.byref(s), t)
+
+
+def make_lclt(xs, ys, z5, lo, hi) -> Integrand:
+    """LC_LT over the box [lo, hi] in (lt, zt, lc): five tables on the grid
+    (xs = lt knots, ys = zt knots), z5 = (tau, mu, sigma, fmsk, fprj)."""
+    T = TablesC()
+    keep = []
+    for q in range(5):
+        g = interp2d(xs, ys, z5[q])
+        keep.append(g)
+        T.lclt[q] = g
+    f = make_integrand(LCLT, 3, 0.0, 0.0, lo=lo, hi=hi)
+    f.tables = C.cast(C.pointer(T), C.c_void_p)
+    f._keep = (T, keep)
+    return f
+
+
+def make_table7(spline_x, spline_y, grid_x, grid_y, grid_z, sigma, offset) -> Integrand:
+    """The 7-D table integrand over [0,1]^7 with one mu offset."""
+    T = TablesC()
+    sp = spline1d(spline_x, spline_y)
+    gr = interp2d(grid_x, grid_y, grid_z)
+    T.spline = sp
+    T.grid = gr
+    T.sigma = float(sigma)
+    T.offset = float(offset)
+    f = make_integrand(TABLE7, 7, 0.0, 0.0)
+    f.tables = C.cast(C.pointer(T), C.c_void_p)
+    f._keep = (T, sp, gr)
+    return f

@@ -464,3 +464,36 @@ def test_reference_style_functor_front_end(oracle):
         assert abs(r["nregions"] - r_c["nregions"]) <= 0.02 * r_c["nregions"] + 4
         if r_c["phase2_regions"] == 0:
             assert r["neval"] == r["nregions"] * oracle.Rule(3).npoints
+
+
+def test_lclt_matches_oracle(cub, oracle, ctx):
+    """The reference's LC_LT integrand (FP64 tables) over its 3-D box."""
+    from cubature import tables as T
+
+    d = T.lclt_data(0)
+    lo, hi = [1.0, 0.1, 0.0], [100.0, 0.3, 6.0]
+    eps = 1e-6
+    f_c = oracle.make_lclt(d["xs"], d["ys"], d["z"], lo, hi)
+    r_c = oracle.Rule(3).integrate_reference(f_c, eps, 1e-12)
+    tab = T.LcLtTables(d, 0)
+    r_g = ctx.integrate_lclt(tab, lo, hi, eps, 1e-12)
+    _compare_full(r_g, r_c, r_c["value"], eps, "lclt")
+
+
+def test_table7_batch_matches_oracle(cub, oracle, ctx):
+    """The 7-D spline x bilinear x Gaussian-kernel integrand, one mu offset
+    per integral, breadth-first with the reference's classification."""
+    from cubature import tables as T
+
+    d = T.table7_data(0)
+    offs = T.table7_offsets(3)
+    eps = 1e-4
+    tab = T.Table7(d, 0)
+    out = ctx.integrate_table7_batch(tab, offs, eps, 1e-12,
+                                     cub.options(policy=cub.POLICY_BREADTH))
+    R = oracle.Rule(7)
+    for r_g, o in zip(out, offs):
+        f_c = oracle.make_table7(d["spline_x"], d["spline_y"], d["grid_x"], d["grid_y"],
+                                 d["grid_z"], d["sigma"], o)
+        r_c = R.integrate_reference(f_c, eps, 1e-12, phase1_cap=1 << 28)
+        _compare_full(r_g, r_c, r_c["value"], eps, ("table7", o))
