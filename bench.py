@@ -327,9 +327,10 @@ def main() -> int:
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     workload = dict(WORKLOADS[args.workload])
-    if args.count and "batch" in workload:
-        fam, n, _ = workload["batch"]
-        workload["batch"] = (fam, n, args.count)
+    for key in ("batch", "tables"):
+        if args.count and key in workload:
+            fam, n, _ = workload[key]
+            workload[key] = (fam, n, args.count)
     world, rank, local = dist_setup()
 
     if args.impl == "reference":

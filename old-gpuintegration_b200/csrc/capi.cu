@@ -282,75 +282,39 @@ int integrate_impl(cub_ctx* ctx, int family, int ndim, int count, const cub_genz
   }
   Options o = to_options(opt);
   if (o.max_slots <= 0) o.max_slots = ctx->ws->auto_slots(ndim, o.policy);
-  std::vector<Result> res(count);
-  // Groups of integrals that share one region list.  Under the reference
-  // policy an integral's list never exceeds its phase-1 cap, so groups of
-  // max_slots / (2 cap + 96) always fit (the driver needs room for 2 n + 32
-  // per integral).  Under the breadth policy lists are unbounded: the whole
-  // batch is tried at once and integrals that were still running when the
-  // capacity ran out are integrated again in groups a quarter the size
-  // (integrals are independent, so a rerun gives the same result).
-  int group = count;
-  if (o.policy == kPolicyReference && o.phase1_cap > 0) {
-    const long long per = 2ll * o.phase1_cap + 96;
-    group = (int)std::max<long long>(1, std::min<long long>(count, o.max_slots / per));
-  }
-  std::vector<int> todo(count);
-  for (int k = 0; k < count; ++k) todo[k] = k;
+  std::vector<Result> res;
   std::vector<GenzParams> hp;
   std::vector<double> ger, gea, gbox;
-  std::vector<Result> gres;
-  int rc = 0;
-  while (!todo.empty()) {
-    std::vector<int> again;
-    for (size_t g0 = 0; g0 < todo.size(); g0 += group) {
-      const int gn = (int)std::min<size_t>(group, todo.size() - g0);
-      hp.resize(gn);
-      ger.resize(gn);
-      gea.resize(gn);
-      gres.assign(gn, Result());
-      for (int j = 0; j < gn; ++j) {
-        const int k = todo[g0 + j];
-        hp[j] = h[k];
-        ger[j] = er[k];
-        gea[j] = ea[k];
-      }
-      if (lo) {
-        // per integral: lo[ndim] then hi[ndim]
-        gbox.resize((size_t)gn * 2 * ndim);
-        for (int j = 0; j < gn; ++j) {
-          const int k = todo[g0 + j];
-          for (int d = 0; d < ndim; ++d) {
-            gbox[(size_t)j * 2 * ndim + d] = lo[(size_t)k * ndim + d];
-            gbox[(size_t)j * 2 * ndim + ndim + d] = hi[(size_t)k * ndim + d];
-          }
-        }
-      }
-      const GenzParams* d = nullptr;
-      if (gn > 1) {
-        if ((e = cudaMemcpyAsync(ctx->d_params, hp.data(), sizeof(GenzParams) * gn,
-                                 cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess)
-          return cuda_fail(e, "cudaMemcpyAsync(params)");
-        ctx->ws->stats().h2d_bytes += (long long)(sizeof(GenzParams) * gn);
-        d = ctx->d_params;
-      }
-      const int r = dispatch_run(ctx, family, ndim, gn, hp.data(), d, ger.data(), gea.data(), o,
-                                 gres.data(), lo ? gbox.data() : nullptr);
-      if (r != 0 && r != kErrCapacity) {
-        rc = r;
-        break;
-      }
-      for (int j = 0; j < gn; ++j) {
-        const int k = todo[g0 + j];
-        res[k] = gres[j];
-        if (r == kErrCapacity && group > 1 && gres[j].state == kStateRunning) again.push_back(k);
-      }
-      if (r == kErrCapacity && (group == 1 || again.empty())) rc = kErrCapacity;
+  const int rc = grouped_batch(count, o, [&](const std::vector<int>& idx, Result* gout) {
+    const int gn = (int)idx.size();
+    hp.resize(gn);
+    ger.resize(gn);
+    gea.resize(gn);
+    for (int j = 0; j < gn; ++j) {
+      hp[j] = h[idx[j]];
+      ger[j] = er[idx[j]];
+      gea[j] = ea[idx[j]];
     }
-    if (rc != 0 && rc != kErrCapacity) break;
-    todo.swap(again);
-    group = std::max(1, group / 4);
-  }
+    if (lo) {
+      // per integral: lo[ndim] then hi[ndim]
+      gbox.resize((size_t)gn * 2 * ndim);
+      for (int j = 0; j < gn; ++j)
+        for (int d = 0; d < ndim; ++d) {
+          gbox[(size_t)j * 2 * ndim + d] = lo[(size_t)idx[j] * ndim + d];
+          gbox[(size_t)j * 2 * ndim + ndim + d] = hi[(size_t)idx[j] * ndim + d];
+        }
+    }
+    const GenzParams* d = nullptr;
+    if (gn > 1) {
+      if (cudaMemcpyAsync(ctx->d_params, hp.data(), sizeof(GenzParams) * gn,
+                          cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess)
+        return (int)kErrCuda;
+      ctx->ws->stats().h2d_bytes += (long long)(sizeof(GenzParams) * gn);
+      d = ctx->d_params;
+    }
+    return dispatch_run(ctx, family, ndim, gn, hp.data(), d, ger.data(), gea.data(), o, gout,
+                        lo ? gbox.data() : nullptr);
+  }, res);
   if (rc == kErrCuda) {
     set_error(ctx->ws->error());
     return CUB_ERR_CUDA;

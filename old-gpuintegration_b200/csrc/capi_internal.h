@@ -3,7 +3,9 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <string>
+#include <vector>
 
 #include "cubature.h"
 #include "cubature/engine.cuh"
@@ -50,6 +52,48 @@ CUB_DECLARE_DIM(6)
 CUB_DECLARE_DIM(7)
 CUB_DECLARE_DIM(8)
 #undef CUB_DECLARE_DIM
+
+// Integrate `count` independent integrals in groups that share one region
+// list.  run(idx, out) integrates the integrals idx (indices into the batch)
+// and returns an engine code.  Under the reference policy an integral's list
+// stays below 2 * phase1_cap + 96 slots, so groups of max_slots / that size
+// always fit.  Under the breadth policy lists are unbounded: the whole batch
+// is tried at once and integrals still running when the capacity ran out are
+// integrated again in groups a quarter the size (integrals are independent,
+// so a rerun gives the same result).  Returns kOk, kErrCapacity (some
+// integral never fit; its result is the last estimate) or the first error.
+template <class Run>
+int grouped_batch(int count, const Options& o, Run&& run, std::vector<Result>& res) {
+  res.assign(count, Result());
+  int group = count;
+  if (o.policy == kPolicyReference && o.phase1_cap > 0) {
+    const long long per = 2ll * o.phase1_cap + 96;
+    group = (int)std::max<long long>(1, std::min<long long>(count, o.max_slots / per));
+  }
+  std::vector<int> todo(count), idx;
+  for (int k = 0; k < count; ++k) todo[k] = k;
+  std::vector<Result> gres;
+  int rc = kOk;
+  while (!todo.empty()) {
+    std::vector<int> again;
+    for (size_t g0 = 0; g0 < todo.size(); g0 += group) {
+      const int gn = (int)std::min<size_t>(group, todo.size() - g0);
+      idx.assign(todo.begin() + g0, todo.begin() + g0 + gn);
+      gres.assign(gn, Result());
+      const int r = run(idx, gres.data());
+      if (r != kOk && r != kErrCapacity) return r;
+      for (int j = 0; j < gn; ++j) {
+        res[idx[j]] = gres[j];
+        if (r == kErrCapacity && group > 1 && gres[j].state == kStateRunning)
+          again.push_back(idx[j]);
+      }
+      if (r == kErrCapacity && (group == 1 || again.empty())) rc = kErrCapacity;
+    }
+    todo.swap(again);
+    group = std::max(1, group / 4);
+  }
+  return rc;
+}
 
 }  // namespace capi
 }  // namespace cubature

@@ -111,19 +111,13 @@ int cub_integrate_table7_batch(cub_ctx* ctx, const cub_table7* tables, int count
   if (e != cudaSuccess) return cuda_error(e, "cudaSetDevice");
   Options o = to_options(opt);
   if (o.max_slots <= 0) o.max_slots = ctx->ws->auto_slots(7, o.policy);
-  // groups that always fit the region list (reference policy: an integral's
-  // list stays below 2 * phase1_cap + 96 slots)
-  int group = count;
-  if (o.policy == kPolicyReference && o.phase1_cap > 0)
-    group = (int)std::max<long long>(
-        1, std::min<long long>(count, o.max_slots / (2ll * o.phase1_cap + 96)));
-  if (group > ctx->aux_cap) {
+  if (count > ctx->aux_cap) {
     if (ctx->d_aux) cudaFree(ctx->d_aux);
     ctx->d_aux = nullptr;
     ctx->aux_cap = 0;
-    if ((e = cudaMalloc(&ctx->d_aux, sizeof(double) * group)) != cudaSuccess)
+    if ((e = cudaMalloc(&ctx->d_aux, sizeof(double) * count)) != cudaSuccess)
       return cuda_error(e, "cudaMalloc(offsets)");
-    ctx->aux_cap = group;
+    ctx->aux_cap = count;
   }
   detail::Table7Source src;
   src.base.spline = Spline1D{tables->spline.xs, tables->spline.ys, tables->spline.y2,
@@ -133,18 +127,24 @@ int cub_integrate_table7_batch(cub_ctx* ctx, const cub_table7* tables, int count
   src.base.inv2s2 = 1.0 / (2.0 * tables->sigma * tables->sigma);
   src.base.offset = 0;
   src.offsets = ctx->d_aux;
-  std::vector<Result> res(group);
-  int worst = kOk;
-  for (int g0 = 0; g0 < count; g0 += group) {
-    const int gn = std::min(group, count - g0);
-    if ((e = cudaMemcpyAsync(ctx->d_aux, offsets + g0, sizeof(double) * gn,
-                             cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess)
-      return cuda_error(e, "cudaMemcpyAsync(offsets)");
-    const int rc = run_batch<7>(*ctx->ws, src, gn, er.data() + g0, ea.data() + g0, o, res.data(),
-                                ctx->stream);
-    if (rc != kOk && rc != kErrCapacity) return engine_status(ctx, rc);
-    if (rc == kErrCapacity) worst = rc;
-    for (int j = 0; j < gn; ++j) result_to_c(res[j], &out[g0 + j]);
-  }
-  return engine_status(ctx, worst);
+  std::vector<double> goff, ger, gea;
+  std::vector<Result> res;
+  const int rc = grouped_batch(count, o, [&](const std::vector<int>& idx, Result* gout) {
+    const int gn = (int)idx.size();
+    goff.resize(gn);
+    ger.resize(gn);
+    gea.resize(gn);
+    for (int j = 0; j < gn; ++j) {
+      goff[j] = offsets[idx[j]];
+      ger[j] = er[idx[j]];
+      gea[j] = ea[idx[j]];
+    }
+    if (cudaMemcpyAsync(ctx->d_aux, goff.data(), sizeof(double) * gn, cudaMemcpyHostToDevice,
+                        ctx->stream) != cudaSuccess)
+      return (int)kErrCuda;
+    return run_batch<7>(*ctx->ws, src, gn, ger.data(), gea.data(), o, gout, ctx->stream);
+  }, res);
+  if (rc != kOk && rc != kErrCapacity) return engine_status(ctx, rc);
+  for (int k = 0; k < count; ++k) result_to_c(res[k], &out[k]);
+  return engine_status(ctx, rc);
 }
