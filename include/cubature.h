@@ -252,6 +252,18 @@ int cub_integrate_table7_batch(cub_ctx* ctx, const cub_table7* tables, int count
                                double epsrel0, double epsabs0, const cub_options* opt,
                                cub_result* out);
 
+/* ---- control-variate network (BF16 tensor cores, tcgen05) ------------ */
+
+/* D[e] = A[e] * B[e]^T on the tensor cores for e < batch: A is m x k, B is
+ * n x k, both bf16 and K-major (row-major with leading dimensions lda, ldb,
+ * multiples of 8), D is m x n fp32 (ldd); FP32 accumulation.  m a multiple
+ * of 128, k of 16, n = 16 or 128.  Device pointers; consecutive batch
+ * entries are lda * m, ldb * n and ldd * m elements apart.  The building
+ * block of the network's training and inference; no counterpart in the
+ * reference. */
+int cub_mlp_gemm_bf16(int batch, int m, int n, int k, const void* d_a, long long lda,
+                      const void* d_b, long long ldb, float* d_d, long long ldd, void* stream);
+
 /* ---- per-step entry points on caller device buffers ------------------ */
 
 /* Rule tables of the degree-9 rule for ndim (GPUQuadRule.cu:31-228):

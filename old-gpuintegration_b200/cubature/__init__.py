@@ -109,7 +109,7 @@ EXPORTS = (
     "cub_ctx_stream", "cub_ctx_stats", "cub_ctx_reset_stats", "cub_ctx_set_timing",
     "cub_ctx_release", "cub_split_noalloc", "cub_ctx_trace", "cub_integrate_box",
     "cub_integrate_batch_box", "cub_spline_second_derivatives", "cub_integrate_lclt",
-    "cub_integrate_table7_batch",
+    "cub_integrate_table7_batch", "cub_mlp_gemm_bf16",
 )
 
 _lib = None
@@ -149,6 +149,8 @@ def load_library(path: str | Path | None = None):
                                      C.POINTER(CResult)]
     L.cub_integrate_table7_batch.argtypes = [vp, vp, C.c_int, dp, dp, dp, C.c_double, C.c_double,
                                              C.POINTER(COptions), C.POINTER(CResult)]
+    L.cub_mlp_gemm_bf16.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, vp, C.c_longlong, vp,
+                                    C.c_longlong, vp, C.c_longlong, vp]
     L.cub_ctx_stream.argtypes = [vp]
     L.cub_ctx_stream.restype = vp
     L.cub_ctx_stats.argtypes = [vp, C.POINTER(CStats)]
@@ -568,3 +570,19 @@ def reduce(avg, err, active, stream=None):
     _check(L.cub_reduce(n, _ptr(avg), _ptr(err), _ptr(active), _ptr(out), _ptr(scratch),
                         scratch.numel(), _stream_ptr(stream)))
     return out
+
+
+def mlp_gemm_bf16(a, b):
+    """D = A @ B^T on the tensor cores (tcgen05): a [batch, m, k] and
+    b [batch, n, k] bf16 CUDA tensors -> fp32 [batch, m, n]."""
+    import torch
+
+    a = a.contiguous()
+    b = b.contiguous()
+    batch, m, k = a.shape
+    n = b.shape[1]
+    d = torch.empty(batch, m, n, dtype=torch.float32, device=a.device)
+    _check(load_library().cub_mlp_gemm_bf16(batch, m, n, k, a.data_ptr(), k, b.data_ptr(), k,
+                                            d.data_ptr(), n,
+                                            torch.cuda.current_stream(a.device).cuda_stream))
+    return d
