@@ -66,6 +66,13 @@ WORKLOADS = {
     "table7_7d_batch": {
         "tables": ("table7", 7, 256), "epsrel": 1e-6, "epsabs": 1e-12, "policy": "breadth",
     },
+    # learned control variate on 7-D product peaks (the batch generator at
+    # n = 7): network trained on the tensor cores, integral of f - g plus
+    # integral of g, plain method as fallback and judge; the plain method's
+    # rate on the same integrands is measured in the same run
+    "cv_productpeak_7d_batch": {
+        "cv": ("product_peak", 7, 256), "epsrel": 1e-6, "epsabs": 1e-12, "policy": "breadth",
+    },
 }
 
 # Algorithmic FP64 flops per integrand evaluation, FMA = 2 (transcendental
@@ -218,7 +225,7 @@ def cpu_reference_rate(workload: dict, seconds: float, threads: int = 0):
         for fam, n, a, u in workload["items"]:
             jobs.append((fam, n, a, u))
     else:
-        fam, n, count = workload["batch"]
+        fam, n, count = workload["batch"] if "batch" in workload else workload["cv"]
         for a, u in product_peak_params(n, count):
             jobs.append((fam, n, a, u))
     rules = {}
@@ -327,7 +334,7 @@ def main() -> int:
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     workload = dict(WORKLOADS[args.workload])
-    for key in ("batch", "tables"):
+    for key in ("batch", "tables", "cv"):
         if args.count and key in workload:
             fam, n, _ = workload[key]
             workload[key] = (fam, n, args.count)
@@ -367,6 +374,27 @@ def main() -> int:
 
         for f in items:
             exact.append(O.exact(O.make_integrand(f.family, f.ndim, f.a, f.u)))
+    elif "cv" in workload:
+        from cubature.parallel import shard_bounds
+
+        fam, n, count = workload["cv"]
+        a0, b0 = shard_bounds(world * count, world, rank)
+        cases = product_peak_params(n, world * count)[a0:b0]
+        plist = [cub.make_params(n, a, u) for a, u in cases]
+        cv_stats = {}
+
+        def step():
+            res, st_cv = ctx.cv_integrate_batch(fam, plist, workload["epsrel"], workload["epsabs"])
+            cv_stats.update(st_cv)
+            return res
+
+        def plain_step():
+            return ctx.integrate_batch(fam, n, plist, workload["epsrel"], workload["epsabs"], opts)
+
+        fams = [(fam, n)] * len(plist)
+        import oracle as O
+
+        exact = [O.exact(O.make_integrand(fam, n, a, u)) for a, u in cases]
     elif "tables" in workload:
         from cubature import tables as T
         from cubature.parallel import shard_bounds
@@ -426,6 +454,17 @@ def main() -> int:
             wall_ms.append((t1 - t0) * 1e3)
     ctx.set_timing(False)
     st = ctx.stats()
+    plain_cmp = None
+    if "cv" in workload:
+        # the plain method on the same integrands, same tolerance, one pass
+        torch.cuda.synchronize()
+        p0 = time.perf_counter()
+        plain_res = plain_step()
+        torch.cuda.synchronize()
+        p_s = time.perf_counter() - p0
+        plain_cmp = {"value": len(plain_res) / p_s, "unit": "integrals/s",
+                     "regions": int(sum(r.nregions for r in plain_res)),
+                     "cv_stats": dict(cv_stats)}
 
     # correctness of the last step against the analytic integrals
     nint = len(results)
@@ -508,6 +547,8 @@ def main() -> int:
             "clocks": clocks.summary(),
             "check": {"integrals": nint, "failed": bad},
         }
+        if plain_cmp is not None:
+            line["plain_same_integrands"] = plain_cmp
         print(json.dumps(line), flush=True)
     ctx.close()
     if pg:

@@ -264,6 +264,68 @@ int cub_integrate_table7_batch(cub_ctx* ctx, const cub_table7* tables, int count
 int cub_mlp_gemm_bf16(int batch, int m, int n, int k, const void* d_a, long long lda,
                       const void* d_b, long long ldb, float* d_d, long long ldd, void* stream);
 
+/* The control-variate networks: `count` independent MLPs g: [0,1]^7 -> R,
+ * 7 -> 128 -> 128 -> 128 -> 1 with SiLU, BF16 weights and activations,
+ * FP32 accumulation on the tensor cores, FP32 master parameters and Adam.
+ * Each network has `samples` training points (a multiple of `batch`, itself
+ * a multiple of 128).  Parameters are initialised from `seed`.  No
+ * counterpart in the reference. */
+#define CUB_MLP_PARAMS 35336 /* fp32 parameters per network (with padding) */
+typedef struct cub_mlp cub_mlp;
+cub_mlp* cub_mlp_create(int device, int count, int samples, int batch, unsigned long long seed);
+void cub_mlp_destroy(cub_mlp* m);
+/* Training data on the device: x [count][samples][7] in [0,1] and
+ * y [count][samples] (fp64).  Targets are scaled by 1 / max|y| per network;
+ * inputs are mapped to 2 x - 1. */
+int cub_mlp_set_data(cub_mlp* m, const double* d_x, const double* d_y);
+/* Host copy of the parameters [count][CUB_MLP_PARAMS]: read (set = 0) or
+ * write (set = 1). */
+int cub_mlp_params(cub_mlp* m, float* h_params, int set);
+/* Forward and backward pass of minibatch b without an update: loss
+ * [count] (mean squared error of the scaled targets) and gradients
+ * [count][CUB_MLP_PARAMS] (host; either may be NULL). */
+int cub_mlp_grad(cub_mlp* m, int b, float* h_loss, float* h_grads);
+/* `epochs` passes of Adam over the data; loss [count] of the last
+ * minibatch (host, may be NULL). */
+int cub_mlp_train(cub_mlp* m, int epochs, float lr, float* h_loss);
+/* g at n points per network: d_x [count][n][7] in [0,1] -> d_g [count][n]
+ * (device, fp64, in the units of the targets). */
+int cub_mlp_eval(cub_mlp* m, long long n, const double* d_x, double* d_g);
+
+/* Learned control variate (7-D): for each integral, a coarse plain run
+ * (epsrel coarse_epsrel; the judge), a network trained on f at `samples`
+ * rule nodes of the initial grid, then the integral of (f - g) and of g,
+ * each adaptively to half the absolute tolerance max(epsrel |I|, epsabs).
+ * The plain method takes over for an integral whose training residual
+ * |f - g| / |f| exceeds rho_max, or whose control-variate result is not
+ * converged or disagrees with the coarse run beyond three times their
+ * error estimates.  Breadth-first refinement throughout.  No counterpart in
+ * the reference. */
+typedef struct cub_cv_options {
+  int samples;           /* training points per integral (default 8192) */
+  int batch;             /* minibatch (default 1024)                     */
+  int epochs;            /* Adam epochs (default 30)                     */
+  float lr;              /* Adam step (default 2e-3)                     */
+  double rho_max;        /* residual ratio above which the plain method
+                            runs instead (default 0.5)                   */
+  double coarse_epsrel;  /* tolerance of the judging plain run (1e-3)    */
+  unsigned long long seed;
+} cub_cv_options;
+
+typedef struct cub_cv_stats {
+  double ms_coarse, ms_train, ms_integrate;  /* wall time of the stages   */
+  int fallbacks;          /* integrals done by the plain method          */
+  int rejected;           /* of which the judge rejected the CV result   */
+  double mean_residual_ratio;
+  unsigned long long regions_residual;  /* regions of the (f - g) runs  */
+  unsigned long long regions_network;   /* regions of the g runs        */
+} cub_cv_stats;
+
+void cub_cv_default_options(cub_cv_options* opt);
+int cub_cv_integrate_batch(cub_ctx* ctx, int family, int count, const cub_genz_params* params,
+                           double epsrel, double epsabs, const cub_cv_options* opt,
+                           cub_result* out, cub_cv_stats* stats);
+
 /* ---- per-step entry points on caller device buffers ------------------ */
 
 /* Rule tables of the degree-9 rule for ndim (GPUQuadRule.cu:31-228):

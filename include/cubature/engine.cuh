@@ -460,13 +460,23 @@ inline void launch_eval(const Src& src, const RuleTables& T, const EngineArgs& a
   k_eval<N, K, Src><<<(unsigned)blocks, 256, 0, s>>>(src, T, a);
 }
 
+// Rule evaluation step of the multi-launch driver when the caller supplies
+// its own (NoHook: the engine's k_eval).  A hook's eval(args, n, stream)
+// evaluates the n slots of the current list into args.avg/err/axis/active
+// and returns 0 or an error code; with a hook the persistent kernel is not
+// used.
+struct NoHook {
+  static constexpr bool kActive = false;
+  int eval(const EngineArgs&, long long, cudaStream_t) const { return 0; }
+};
+
 // Run one batch: `nint` integrals of one family and dimension N, each over
 // its box (h_box[k] = lo[N] then hi[N], host memory; the unit cube when
 // h_box is null).  Results go to out[0..nint).
-template <int N, class Src>
+template <int N, class Src, class Hook = NoHook>
 int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
               const double* epsabs, const Options& opt, Result* out, cudaStream_t s,
-              const double* h_box = nullptr) {
+              const double* h_box = nullptr, const Hook& hook = Hook()) {
   static_assert(N >= 2 && N <= kMaxDim, "dimension out of range");
   const long long max_slots = opt.max_slots > 0 ? opt.max_slots : ws.auto_slots(N, opt.policy);
   if (nint <= 0) return kErrInvalid;
@@ -553,7 +563,7 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
 
   // persistent kernel geometry (queried once per device and instantiation)
   int pblocks = 0;
-  if (opt.persistent) {
+  if (opt.persistent && !Hook::kActive) {
     static int per_sm_cache[64];
     static bool cached[64];
     const int dev = ws.device() & 63;
@@ -682,10 +692,15 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
     int K = opt.lanes;
     if (K <= 0) K = n_cur >= (long long)sms * 512 ? 1 : (n_cur >= (long long)sms * 64 ? 8 : 32);
     if (ws.timing) ws.ck(cudaEventRecord(ws.ev[0], s));
-    switch (K) {
-      case 1: launch_eval<N, 1>(src, T, a, sms, s); break;
-      case 8: launch_eval<N, 8>(src, T, a, sms, s); break;
-      default: launch_eval<N, 32>(src, T, a, sms, s); break;
+    if constexpr (Hook::kActive) {
+      const int hr = hook.eval(a, n_cur, s);
+      if (hr) return hr;
+    } else {
+      switch (K) {
+        case 1: launch_eval<N, 1>(src, T, a, sms, s); break;
+        case 8: launch_eval<N, 8>(src, T, a, sms, s); break;
+        default: launch_eval<N, 32>(src, T, a, sms, s); break;
+      }
     }
     if (ws.timing) ws.ck(cudaEventRecord(ws.ev[1], s));
     st.eval_launches += 1;

@@ -35,7 +35,7 @@ __device__ __forceinline__ float silu_grad(float z) {
   return s * (1.0f + z * (1.0f - s));
 }
 
-enum Epilogue : int { kEpiStore = 0, kEpiForward = 1, kEpiBackward = 2 };
+enum Epilogue : int { kEpiStore = 0, kEpiForward = 1, kEpiBackward = 2, kEpiInfer = 3 };
 
 struct EpiArgs {
   // kEpiStore: out[e * batch_out + row * ld_out + col] (fp32)
@@ -71,6 +71,14 @@ __device__ __forceinline__ void epilogue(const EpiArgs& ep, int e, int row, int 
       ep.z[ra + i] = zb;
       ep.h[ra + i] = hb;
       ep.ht[rt + (long long)(c0 + i) * ep.ld_t] = hb;
+    }
+  } else if (EPI == kEpiInfer) {
+    // forward without the training copies: H only (same roundings)
+    const float* b = ep.bias + (long long)e * ep.batch_bias + c0;
+    const long long ra = (long long)e * ep.batch_act + (long long)row * ep.ld_act + c0;
+    for (int i = 0; i < cnt; ++i) {
+      const __nv_bfloat16 zb = __float2bfloat16(v[i] + b[i]);
+      ep.h[ra + i] = __float2bfloat16(silu(__bfloat162float(zb)));
     }
   } else {
     const long long ra = (long long)e * ep.batch_act + (long long)row * ep.ld_act + c0;
@@ -137,6 +145,181 @@ __global__ void __launch_bounds__(128) k_gemm(umma::GemmArgs g, EpiArgs ep) {
   umma::fence_before_sync();
   __syncthreads();
   if (threadIdx.x < 32) umma::tmem_dealloc(tmem, kCols);
+}
+
+// Layout of one network's fp32 parameter vector (also of its gradient and
+// Adam moments).  W0 is [128][16] (out-major; inputs 7..15 are padding and
+// stay zero), W1, W2 are [128][128] (out-major), w3 the output weights.
+struct Layout {
+  static constexpr int W0 = 0;
+  static constexpr int B0 = W0 + kHidden * kInPad;
+  static constexpr int W1 = B0 + kHidden;
+  static constexpr int B1 = W1 + kHidden * kHidden;
+  static constexpr int W2 = B1 + kHidden;
+  static constexpr int B2 = W2 + kHidden * kHidden;
+  static constexpr int W3 = B2 + kHidden;
+  static constexpr int B3 = W3 + kHidden;
+  static constexpr int kCount = B3 + 8;  // padded to 8 floats
+};
+
+// Inputs of network e: x in [0,1]^7 (fp64, [count][7]) -> bf16 (2x - 1),
+// padded to 16, row-major X [count][16] and transposed XT [16][ld_t].
+__global__ void k_prep_inputs(const double* x, long long count, long long batch_x,
+                              __nv_bfloat16* X, __nv_bfloat16* XT, long long ld_t,
+                              long long batch_X, long long batch_XT) {
+  const int e = blockIdx.z;
+  for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < count;
+       s += (long long)gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int i = 0; i < kInPad; ++i) {
+      const float v = i < kIn ? (float)(2.0 * x[e * batch_x + s * kIn + i] - 1.0) : 0.0f;
+      const __nv_bfloat16 b = __float2bfloat16(v);
+      X[e * batch_X + s * kInPad + i] = b;
+      XT[e * batch_XT + (long long)i * ld_t + s] = b;
+    }
+  }
+}
+
+// Output layer on the CUDA cores, one thread per sample, 128 per block:
+// g = H3 . w3 + b3.  Training (y != null): err = g - y; dZ3 = e w3 silu'(Z3)
+// with e = 2 err / nbatch written row-major and transposed, and per-block
+// partials part[blk] = (sum_s e H3[s][:], sum_s e, sum_s err^2).  Inference
+// (g_out != null): g_out[s] = scale * g.
+__global__ void __launch_bounds__(128) k_output(const float* P, const __nv_bfloat16* H3,
+                                                const __nv_bfloat16* Z3, const float* y,
+                                                long long batch_y, float inv_nbatch, __nv_bfloat16* dZ3,
+                                                __nv_bfloat16* dZ3T, float* part,
+                                                long long rows, long long valid,
+                                                const float* scale, double* g_out,
+                                                long long batch_g) {
+  __shared__ float w3[kHidden];
+  __shared__ float es[kHidden];
+  const int e = blockIdx.z;
+  const float* p = P + (long long)e * Layout::kCount;
+  w3[threadIdx.x] = p[Layout::W3 + threadIdx.x];
+  __syncthreads();
+  const long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long base = (long long)e * rows * kHidden;
+  float g = p[Layout::B3];
+  for (int j = 0; j < kHidden; ++j) g += __bfloat162float(H3[base + s * kHidden + j]) * w3[j];
+  if (g_out) {
+    if (s < valid) g_out[(long long)e * batch_g + s] = (double)scale[e] * (double)g;
+    return;
+  }
+  const float err = g - y[(long long)e * batch_y + s];
+  const float ec = 2.0f * err * inv_nbatch;
+  es[threadIdx.x] = ec;
+  for (int j = 0; j < kHidden; ++j) {
+    const float dz = ec * w3[j] * silu_grad(__bfloat162float(Z3[base + s * kHidden + j]));
+    const __nv_bfloat16 b = __float2bfloat16(dz);
+    dZ3[base + s * kHidden + j] = b;
+    dZ3T[base + (long long)j * rows + s] = b;
+  }
+  __syncthreads();
+  // partial output-layer gradients of this block's 128 samples (fixed order)
+  float* out = part + ((long long)e * gridDim.x + blockIdx.x) * (kHidden + 2);
+  const long long s0 = (long long)blockIdx.x * blockDim.x;
+  float acc = 0;
+  for (int i = 0; i < 128; ++i)
+    acc += es[i] * __bfloat162float(H3[base + (s0 + i) * kHidden + threadIdx.x]);
+  out[threadIdx.x] = acc;
+  // error sum and squared error, reduced by thread 0 in order
+  __shared__ float sq[kHidden];
+  sq[threadIdx.x] = err * err;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float se = 0, ss = 0;
+    for (int i = 0; i < 128; ++i) {
+      se += es[i];
+      ss += sq[i];
+    }
+    out[kHidden] = se;
+    out[kHidden + 1] = ss;
+  }
+}
+
+// Sum the per-block partials in block order: gradients of w3 and b3, and
+// the mean squared error of the batch.
+__global__ void k_reduce_output(const float* part, int nblk, float* G, float* loss,
+                                float inv_nbatch) {
+  const int e = blockIdx.z;
+  const float* pe = part + (long long)e * nblk * (kHidden + 2);
+  for (int j = threadIdx.x; j < kHidden + 2; j += blockDim.x) {
+    float a = 0;
+    for (int b = 0; b < nblk; ++b) a += pe[(long long)b * (kHidden + 2) + j];
+    if (j < kHidden)
+      G[(long long)e * Layout::kCount + Layout::W3 + j] = a;
+    else if (j == kHidden)
+      G[(long long)e * Layout::kCount + Layout::B3] = a;
+    else
+      loss[e] = a * inv_nbatch;
+  }
+}
+
+// Bias gradients: G[off + j] = sum_s dZT[j][s], a warp per j (fixed order).
+__global__ void k_bias_grad(const __nv_bfloat16* dZT, long long rows, float* G, int off) {
+  const int e = blockIdx.z;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (warp >= kHidden) return;
+  const __nv_bfloat16* r = dZT + ((long long)e * kHidden + warp) * rows;
+  float a = 0;
+  for (long long s = lane; s < rows; s += 32) a += __bfloat162float(r[s]);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+  if (lane == 0) G[(long long)e * Layout::kCount + off + warp] = a;
+}
+
+// Adam on every parameter of every network (step t >= 1, bias-corrected).
+__global__ void k_adam(float* P, const float* G, float* M, float* V, long long n, float lr,
+                       float b1, float b2, float eps, float c1, float c2) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const float g = G[i];
+    const float m = b1 * M[i] + (1 - b1) * g;
+    const float v = b2 * V[i] + (1 - b2) * g * g;
+    M[i] = m;
+    V[i] = v;
+    P[i] -= lr * (m / c1) / (sqrtf(v / c2) + eps);
+  }
+}
+
+// bf16 copies of the weights for the tensor cores: W0, W1, W2 (out-major)
+// and W1T, W2T (in-major).
+__global__ void k_refresh_weights(const float* P, __nv_bfloat16* W0, __nv_bfloat16* W1,
+                                  __nv_bfloat16* W1T, __nv_bfloat16* W2, __nv_bfloat16* W2T) {
+  const int e = blockIdx.z;
+  const float* p = P + (long long)e * Layout::kCount;
+  const long long sq = (long long)kHidden * kHidden;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kHidden * kHidden;
+       i += gridDim.x * blockDim.x) {
+    const int r = i / kHidden, c = i % kHidden;
+    const __nv_bfloat16 w1 = __float2bfloat16(p[Layout::W1 + i]);
+    const __nv_bfloat16 w2 = __float2bfloat16(p[Layout::W2 + i]);
+    W1[e * sq + i] = w1;
+    W2[e * sq + i] = w2;
+    W1T[e * sq + (long long)c * kHidden + r] = w1;
+    W2T[e * sq + (long long)c * kHidden + r] = w2;
+    if (i < kHidden * kInPad)
+      W0[(long long)e * kHidden * kInPad + i] = __float2bfloat16(p[Layout::W0 + i]);
+  }
+}
+
+// Targets of network e scaled by 1 / max |y| (scale[e] = max |y|, 1 if 0).
+__global__ void k_scale_targets(const double* y, long long count, float* Y, float* scale) {
+  const int e = blockIdx.z;
+  __shared__ double red[256];
+  double m = 0;
+  for (long long s = threadIdx.x; s < count; s += blockDim.x) m = fmax(m, fabs(y[e * count + s]));
+  red[threadIdx.x] = m;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + o]);
+    __syncthreads();
+  }
+  const double sc = red[0] > 0 ? red[0] : 1.0;
+  if (threadIdx.x == 0) scale[e] = (float)sc;
+  for (long long s = threadIdx.x; s < count; s += blockDim.x)
+    Y[e * count + s] = (float)(y[e * count + s] / sc);
 }
 
 }  // namespace mlp

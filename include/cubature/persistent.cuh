@@ -209,6 +209,22 @@ struct PointTable {
   }
 };
 
+// f(x, p) for functors that take the rule point's index (values computed
+// ahead of the rule, e.g. the control-variate network), else f(x).
+template <class F>
+__device__ __forceinline__ auto call_point_(const F& f, const double* x, int p, int)
+    -> decltype(f(x, p)) {
+  return f(x, p);
+}
+template <class F>
+__device__ __forceinline__ double call_point_(const F& f, const double* x, int, long) {
+  return f(x);
+}
+template <class F>
+__device__ __forceinline__ double call_point(const F& f, const double* x, int p) {
+  return call_point_(f, x, p, 0);
+}
+
 template <int N>
 struct GroupSmem {
   PointTable<N> pt;
@@ -249,7 +265,7 @@ __device__ __forceinline__ RegionResult eval_region_group(const F& f, const doub
     double x[N];
 #pragma unroll
     for (int i = 0; i < N; ++i) x[i] = fma(sm.pt.ctab[(e.x >> (4 * i)) & 15u], H[i], L[i]);
-    const double fx = f(x);
+    const double fx = call_point(f, x, p);
     if (p <= 4 * N) sm.fstage[g][p] = fx;
 #pragma unroll
     for (int k = 0; k < kNumSets; ++k) S[k] += (e.y == (unsigned)k) ? fx : 0.0;

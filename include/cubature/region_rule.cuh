@@ -72,7 +72,7 @@ struct RegionSums {
 
 // Coefficient of the box width for a coordinate with generator value +g
 // (minus = false) or -g (minus = true): x = L + (0.5 - g) H.
-__device__ __forceinline__ constexpr double coef(double g, bool minus) {
+__host__ __device__ __forceinline__ constexpr double coef(double g, bool minus) {
   return minus ? (0.5 + g) : (0.5 - g);
 }
 

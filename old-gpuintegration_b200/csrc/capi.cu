@@ -26,7 +26,7 @@ int engine_status(cub_ctx* ctx, int rc) {
     case kOk:
       return 0;
     case kErrCuda:
-      set_error(ctx->ws->error());
+      if (!ctx->ws->error().empty()) set_error(ctx->ws->error());
       return CUB_ERR_CUDA;
     case kErrTimeout:
       set_error("a device-side grid barrier wait ran out (persistent kernel)");

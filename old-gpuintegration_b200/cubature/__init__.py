@@ -102,6 +102,22 @@ class COptions(C.Structure):
 
 
 #: every symbol include/cubature.h declares
+class CvOptions(C.Structure):
+    _fields_ = [("samples", C.c_int), ("batch", C.c_int), ("epochs", C.c_int), ("lr", C.c_float),
+                ("rho_max", C.c_double), ("coarse_epsrel", C.c_double),
+                ("seed", C.c_ulonglong)]
+
+
+class CvStats(C.Structure):
+    _fields_ = [("ms_coarse", C.c_double), ("ms_train", C.c_double),
+                ("ms_integrate", C.c_double), ("fallbacks", C.c_int), ("rejected", C.c_int),
+                ("mean_residual_ratio", C.c_double), ("regions_residual", C.c_ulonglong),
+                ("regions_network", C.c_ulonglong)]
+
+    def to_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 EXPORTS = (
     "cub_version", "cub_last_error", "cub_default_options", "cub_create", "cub_destroy",
     "cub_ctx_bytes", "cub_integrate", "cub_integrate_batch", "cub_rule_tables", "cub_rule_eval",
@@ -109,7 +125,9 @@ EXPORTS = (
     "cub_ctx_stream", "cub_ctx_stats", "cub_ctx_reset_stats", "cub_ctx_set_timing",
     "cub_ctx_release", "cub_split_noalloc", "cub_ctx_trace", "cub_integrate_box",
     "cub_integrate_batch_box", "cub_spline_second_derivatives", "cub_integrate_lclt",
-    "cub_integrate_table7_batch", "cub_mlp_gemm_bf16",
+    "cub_integrate_table7_batch", "cub_mlp_gemm_bf16", "cub_mlp_create", "cub_mlp_destroy",
+    "cub_mlp_set_data", "cub_mlp_params", "cub_mlp_grad", "cub_mlp_train", "cub_mlp_eval",
+    "cub_cv_default_options", "cub_cv_integrate_batch",
 )
 
 _lib = None
@@ -151,6 +169,18 @@ def load_library(path: str | Path | None = None):
                                              C.POINTER(COptions), C.POINTER(CResult)]
     L.cub_mlp_gemm_bf16.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, vp, C.c_longlong, vp,
                                     C.c_longlong, vp, C.c_longlong, vp]
+    L.cub_mlp_create.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_ulonglong]
+    L.cub_mlp_create.restype = vp
+    L.cub_mlp_destroy.argtypes = [vp]
+    L.cub_mlp_set_data.argtypes = [vp, vp, vp]
+    L.cub_mlp_params.argtypes = [vp, vp, C.c_int]
+    L.cub_mlp_grad.argtypes = [vp, C.c_int, vp, vp]
+    L.cub_mlp_train.argtypes = [vp, C.c_int, C.c_float, vp]
+    L.cub_mlp_eval.argtypes = [vp, C.c_longlong, vp, vp]
+    L.cub_cv_default_options.argtypes = [C.POINTER(CvOptions)]
+    L.cub_cv_integrate_batch.argtypes = [vp, C.c_int, C.c_int, C.POINTER(GenzParams), C.c_double,
+                                         C.c_double, C.POINTER(CvOptions), C.POINTER(CResult),
+                                         C.POINTER(CvStats)]
     L.cub_ctx_stream.argtypes = [vp]
     L.cub_ctx_stream.restype = vp
     L.cub_ctx_stats.argtypes = [vp, C.POINTER(CStats)]
@@ -414,6 +444,22 @@ class Context:
             raise CubatureError(rc, last_error())
         return [Result.from_c(out[i]) for i in range(n)]
 
+    def cv_integrate_batch(self, family, params: Sequence[GenzParams], epsrel: float,
+                           epsabs: float, **cv_opts):
+        """Learned control variate over a batch of 7-D integrals
+        (cub_cv_integrate_batch): (results, stats dict)."""
+        o = CvOptions()
+        self._lib.cub_cv_default_options(C.byref(o))
+        for k, v in cv_opts.items():
+            setattr(o, k, v)
+        n = len(params)
+        arr = (GenzParams * n)(*params)
+        out = (CResult * n)()
+        st = CvStats()
+        _check(self._lib.cub_cv_integrate_batch(self._h, family_id(family), n, arr, epsrel,
+                                                epsabs, C.byref(o), out, C.byref(st)))
+        return [Result.from_c(out[i]) for i in range(n)], st.to_dict()
+
 def spline_second_derivatives(xs, ys):
     """Natural cubic spline second derivatives (host), for device splines."""
     import numpy as np
@@ -586,3 +632,73 @@ def mlp_gemm_bf16(a, b):
                                             d.data_ptr(), n,
                                             torch.cuda.current_stream(a.device).cuda_stream))
     return d
+
+
+MLP_PARAMS = 35336  # CUB_MLP_PARAMS
+
+
+class Mlp:
+    """`count` control-variate networks (cub_mlp_*): 7 -> 128 -> 128 -> 128 -> 1,
+    SiLU, BF16 tensor-core training and inference."""
+
+    def __init__(self, count: int, samples: int, batch: int = 1024, seed: int = 1,
+                 device: int = 0):
+        self._lib = load_library()
+        self.count, self.samples, self.batch = count, samples, batch
+        self._h = self._lib.cub_mlp_create(device, count, samples, batch, seed)
+        if not self._h:
+            raise CubatureError(ERR_CUDA, last_error())
+
+    def close(self):
+        if self._h:
+            self._lib.cub_mlp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_data(self, x, y):
+        """x: [count, samples, 7] and y: [count, samples], float64 CUDA tensors."""
+        x, y = x.contiguous(), y.contiguous()
+        self._keep = (x, y)
+        _check(self._lib.cub_mlp_set_data(self._h, x.data_ptr(), y.data_ptr()))
+
+    def params(self):
+        import numpy as np
+
+        p = np.zeros((self.count, MLP_PARAMS), dtype=np.float32)
+        _check(self._lib.cub_mlp_params(self._h, p.ctypes.data, 0))
+        return p
+
+    def set_params(self, p):
+        import numpy as np
+
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        _check(self._lib.cub_mlp_params(self._h, p.ctypes.data, 1))
+
+    def grad(self, b: int = 0):
+        import numpy as np
+
+        loss = np.zeros(self.count, dtype=np.float32)
+        g = np.zeros((self.count, MLP_PARAMS), dtype=np.float32)
+        _check(self._lib.cub_mlp_grad(self._h, b, loss.ctypes.data, g.ctypes.data))
+        return loss, g
+
+    def train(self, epochs: int, lr: float = 1e-3):
+        import numpy as np
+
+        loss = np.zeros(self.count, dtype=np.float32)
+        _check(self._lib.cub_mlp_train(self._h, epochs, lr, loss.ctypes.data))
+        return loss
+
+    def eval(self, x):
+        """x: [count, n, 7] float64 CUDA tensor -> g [count, n] float64."""
+        import torch
+
+        x = x.contiguous()
+        g = torch.empty(x.shape[0], x.shape[1], dtype=torch.float64, device=x.device)
+        _check(self._lib.cub_mlp_eval(self._h, x.shape[1], x.data_ptr(), g.data_ptr()))
+        return g
