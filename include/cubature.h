@@ -198,6 +198,17 @@ int cub_integrate_batch_box(cub_ctx* ctx, int family, int ndim, int count,
                             const double* epsrel, const double* epsabs, double epsrel0,
                             double epsabs0, const cub_options* opt, cub_result* out);
 
+/* Autotuner: integrate the batch (or its first `sample` integrals when
+ * sample > 0) with each candidate tiling -- regions per block of the
+ * persistent kernel (persistent_max_r 1, 2, 4, 8), lanes per region of the
+ * multi-launch rule kernel (1, 8, 32), the persistent kernel on or off and
+ * its hand-over length -- starting from *opt (or the defaults), and write
+ * the fastest to *best; *best_ms receives its time (may be NULL).  Each
+ * candidate runs twice and keeps the faster run. */
+int cub_autotune_batch(cub_ctx* ctx, int family, int ndim, int count,
+                       const cub_genz_params* params, double epsrel, double epsabs, int sample,
+                       const cub_options* opt, cub_options* best, double* best_ms);
+
 /* ---- integrands on device tables ------------------------------------- */
 
 /* Rectilinear 2-D table in device memory, row-major zs[i * ny + j] at

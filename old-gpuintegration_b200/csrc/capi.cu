@@ -1,8 +1,10 @@
 // capi.cu -- the C ABI (include/cubature.h): contexts, dispatch by
 // dimension and family, per-step entry points.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "capi_internal.h"
 #include "cubature/step_kernels.cuh"
@@ -465,3 +467,71 @@ int cub_reduce(long long n, const double* d_avg, const double* d_err, const int*
 }
 
 }  // extern "C"
+
+int cub_autotune_batch(cub_ctx* ctx, int family, int ndim, int count,
+                       const cub_genz_params* params, double epsrel, double epsabs, int sample,
+                       const cub_options* opt, cub_options* best, double* best_ms) {
+  if (!ctx || !params || !best || count <= 0) {
+    set_error("invalid argument");
+    return CUB_ERR_INVALID;
+  }
+  const int n = sample > 0 ? std::min(sample, count) : count;
+  cub_options base;
+  if (opt)
+    base = *opt;
+  else
+    cub_default_options(&base);
+  std::vector<cub_options> cands;
+  for (int r : {1, 2, 4, 8})
+    for (int pm : {0, 4096}) {
+      cub_options c = base;
+      c.no_persistent = 0;
+      c.persistent_max_r = r;
+      c.persistent_max_n = pm;
+      cands.push_back(c);
+    }
+  for (int lanes : {1, 8, 32}) {
+    cub_options c = base;
+    c.no_persistent = 1;
+    c.lanes = lanes;
+    cands.push_back(c);
+  }
+  std::vector<cub_result> out(n);
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
+    return cuda_fail(cudaGetLastError(), "cudaEventCreate");
+  double bt = 1e300;
+  int bi = -1;
+  int rc = 0;
+  for (size_t i = 0; i < cands.size() && rc == 0; ++i) {
+    double t = 1e300;
+    for (int rep = 0; rep < 2; ++rep) {
+      cudaEventRecord(e0, ctx->stream);
+      const int r = cub_integrate_batch(ctx, family, ndim, n, params, nullptr, nullptr, epsrel,
+                                        epsabs, &cands[i], out.data());
+      cudaEventRecord(e1, ctx->stream);
+      if (r < 0 && r != CUB_ERR_CAPACITY) {
+        rc = r;
+        break;
+      }
+      cudaEventSynchronize(e1);
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (r == 0) t = std::min(t, (double)ms);
+    }
+    if (t < bt) {
+      bt = t;
+      bi = (int)i;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  if (bi < 0) {
+    set_error("autotune: no candidate completed the batch");
+    return CUB_ERR_CAPACITY;
+  }
+  *best = cands[bi];
+  if (best_ms) *best_ms = bt;
+  return 0;
+}

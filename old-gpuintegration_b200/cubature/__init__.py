@@ -127,7 +127,7 @@ EXPORTS = (
     "cub_integrate_batch_box", "cub_spline_second_derivatives", "cub_integrate_lclt",
     "cub_integrate_table7_batch", "cub_mlp_gemm_bf16", "cub_mlp_create", "cub_mlp_destroy",
     "cub_mlp_set_data", "cub_mlp_params", "cub_mlp_grad", "cub_mlp_train", "cub_mlp_eval",
-    "cub_cv_default_options", "cub_cv_integrate_batch",
+    "cub_cv_default_options", "cub_cv_integrate_batch", "cub_autotune_batch",
 )
 
 _lib = None
@@ -181,6 +181,9 @@ def load_library(path: str | Path | None = None):
     L.cub_cv_integrate_batch.argtypes = [vp, C.c_int, C.c_int, C.POINTER(GenzParams), C.c_double,
                                          C.c_double, C.POINTER(CvOptions), C.POINTER(CResult),
                                          C.POINTER(CvStats)]
+    L.cub_autotune_batch.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.POINTER(GenzParams),
+                                     C.c_double, C.c_double, C.c_int, C.POINTER(COptions),
+                                     C.POINTER(COptions), C.POINTER(C.c_double)]
     L.cub_ctx_stream.argtypes = [vp]
     L.cub_ctx_stream.restype = vp
     L.cub_ctx_stats.argtypes = [vp, C.POINTER(CStats)]
@@ -459,6 +462,18 @@ class Context:
         _check(self._lib.cub_cv_integrate_batch(self._h, family_id(family), n, arr, epsrel,
                                                 epsabs, C.byref(o), out, C.byref(st)))
         return [Result.from_c(out[i]) for i in range(n)], st.to_dict()
+
+    def autotune_batch(self, family, ndim: int, params: Sequence[GenzParams], epsrel: float,
+                       epsabs: float, sample: int = 0, opts: COptions | None = None):
+        """Fastest tiling for this batch (cub_autotune_batch): (options, ms)."""
+        n = len(params)
+        arr = (GenzParams * n)(*params)
+        best = COptions()
+        ms = C.c_double()
+        _check(self._lib.cub_autotune_batch(self._h, family_id(family), ndim, n, arr, epsrel,
+                                            epsabs, sample, C.byref(opts) if opts else None,
+                                            C.byref(best), C.byref(ms)))
+        return best, ms.value
 
 def spline_second_derivatives(xs, ys):
     """Natural cubic spline second derivatives (host), for device splines."""

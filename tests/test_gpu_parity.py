@@ -497,3 +497,24 @@ def test_table7_batch_matches_oracle(cub, oracle, ctx):
                                  d["grid_z"], d["sigma"], o)
         r_c = R.integrate_reference(f_c, eps, 1e-12, phase1_cap=1 << 28)
         _compare_full(r_g, r_c, r_c["value"], eps, ("table7", o))
+
+
+def test_autotune_picks_a_working_tiling(cub, ctx):
+    """The autotuner returns one of its candidates, and the batch integrated
+    with it gives the default options' answers."""
+    n, eps = 5, 1e-5
+    params = [cub.make_params(n, list(a), list(u)) for a, u in
+              ((a, u) for a, u in _peak_params_np(n, 12, 4))]
+    best, ms = ctx.autotune_batch("product_peak", n, params, eps, 1e-12)
+    assert ms > 0 and best.persistent_max_r in (0, 1, 2, 4, 8) and best.lanes in (0, 1, 8, 32)
+    tuned = ctx.integrate_batch("product_peak", n, params, eps, 1e-12, best)
+    ref = ctx.integrate_batch("product_peak", n, params, eps, 1e-12)
+    for t, r in zip(tuned, ref):
+        assert t.status == r.status
+        assert abs(t.integral - r.integral) <= 1e-3 * eps * abs(r.integral)
+
+
+def _peak_params_np(n, count, seed):
+    rng = np.random.default_rng(seed)
+    return [(np.exp(rng.uniform(0, np.log(20), n)), rng.uniform(0.1, 0.9, n))
+            for _ in range(count)]
