@@ -68,7 +68,7 @@ WORKLOADS = {
     },
     # learned control variate on 7-D product peaks (the batch generator at
     # n = 7): network trained on the tensor cores, integral of f - g plus
-    # integral of g, plain method as fallback and judge; the plain method's
+    # integral of g, plain method as fallback and check; the plain method's
     # rate on the same integrands is measured in the same run
     "cv_productpeak_7d_batch": {
         "cv": ("product_peak", 7, 256), "epsrel": 1e-6, "epsabs": 1e-12, "policy": "breadth",
@@ -365,8 +365,19 @@ def main() -> int:
     if "items" in workload:
         items = [cub.Integrand(f, n, a, u) for f, n, a, u in workload["items"]]
 
-        def step():
+        same_dim = len({f.ndim for f in items}) == 1
+
+        def single_calls():
             return [ctx.integrate(f, workload["epsrel"], workload["epsabs"], opts) for f in items]
+
+        def step():
+            # one public-API call per integrand, the reference's calling
+            # pattern (one mixed-family call, cub_integrate_mixed_batch, is
+            # measured beside it)
+            return single_calls()
+
+        def mixed_call():
+            return ctx.integrate_mixed(items, workload["epsrel"], workload["epsabs"], opts)
 
         fams = [(f.family, f.ndim) for f in items]
         exact = []
@@ -455,6 +466,23 @@ def main() -> int:
     ctx.set_timing(False)
     st = ctx.stats()
     plain_cmp = None
+    single_cmp = None
+    if "items" in workload and len(workload["items"]) > 1 and same_dim:
+        # the same integrals in one mixed-family call, timed the same way
+        ms = []
+        for _ in range(max(3, args.steps)):
+            flush.zero_()
+            torch.cuda.synchronize()
+            s0 = torch.cuda.Event(enable_timing=True)
+            s1 = torch.cuda.Event(enable_timing=True)
+            s0.record(stream)
+            mixed_call()
+            s1.record(stream)
+            torch.cuda.synchronize()
+            ms.append(s0.elapsed_time(s1))
+        single_cmp = {"value": len(items) * len(ms) / (sum(ms) / 1e3), "unit": "integrals/s",
+                      "ms_per_step": sum(ms) / len(ms),
+                      "call": "cub_integrate_mixed_batch, all integrands in one call"}
     if "cv" in workload:
         # the plain method on the same integrands, same tolerance, one pass
         torch.cuda.synchronize()
@@ -549,6 +577,9 @@ def main() -> int:
         }
         if plain_cmp is not None:
             line["plain_same_integrands"] = plain_cmp
+        if single_cmp is not None:
+            line["config"]["call"] = "cub_integrate, one call per integrand"
+            line["mixed_call"] = single_cmp
         print(json.dumps(line), flush=True)
     ctx.close()
     if pg:

@@ -182,6 +182,15 @@ int cub_integrate_batch(cub_ctx* ctx, int family, int ndim, int count,
                         const double* epsabs, double epsrel0, double epsabs0,
                         const cub_options* opt, cub_result* out);
 
+/* `count` integrals of possibly different families (families[k]) and one
+ * dimension, integrated together on one region list -- e.g. the 8-D
+ * oscillatory and corner peak in one persistent launch.  Results are those
+ * of cub_integrate_batch per family (the same arithmetic). */
+int cub_integrate_mixed_batch(cub_ctx* ctx, int ndim, int count, const int* families,
+                              const cub_genz_params* params, const double* epsrel,
+                              const double* epsabs, double epsrel0, double epsabs0,
+                              const cub_options* opt, cub_result* out);
+
 /* cub_integrate over the box [lo, hi] (ndim values each, host memory,
  * finite, hi > lo) instead of the unit cube: the reference's Volume
  * argument (GPUQuadVolume.cu:4-25, GPUQuadSample.cu:44-56,174-179), here in
@@ -304,7 +313,7 @@ int cub_mlp_train(cub_mlp* m, int epochs, float lr, float* h_loss);
 int cub_mlp_eval(cub_mlp* m, long long n, const double* d_x, double* d_g);
 
 /* Learned control variate (7-D): for each integral, a coarse plain run
- * (epsrel coarse_epsrel; the judge), a network trained on f at `samples`
+ * (epsrel coarse_epsrel; it checks the result), a network trained on f at `samples`
  * rule nodes of the initial grid, then the integral of (f - g) and of g,
  * each adaptively to half the absolute tolerance max(epsrel |I|, epsabs).
  * The plain method takes over for an integral whose training residual
@@ -326,7 +335,7 @@ typedef struct cub_cv_options {
 typedef struct cub_cv_stats {
   double ms_coarse, ms_train, ms_integrate;  /* wall time of the stages   */
   int fallbacks;          /* integrals done by the plain method          */
-  int rejected;           /* of which the judge rejected the CV result   */
+  int rejected;           /* of which the check rejected the CV result   */
   double mean_residual_ratio;
   unsigned long long regions_residual;  /* regions of the (f - g) runs  */
   unsigned long long regions_network;   /* regions of the g runs        */

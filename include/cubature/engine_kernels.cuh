@@ -172,6 +172,16 @@ struct ParamSource {
   __device__ __forceinline__ F get(int k) const { return F::load(params[k]); }
 };
 
+// Integrals of different families in one batch (family per integral).
+template <int N>
+struct MixedSource {
+  const GenzParams* params;
+  const int* families;
+  __device__ __forceinline__ MixedGenz<N> get(int k) const {
+    return MixedGenz<N>::make(params[k], families[k]);
+  }
+};
+
 // Write one region's results (reference classification:
 // fail when err / max(epsrel|avg|, epsabs) > 1, GPUQuadPhases.cu:63-74).
 __device__ __forceinline__ void store_result(const EngineArgs& a, long long slot,

@@ -166,4 +166,45 @@ struct CosSum {
   }
 };
 
+// One integrand of any built-in family, chosen per integral: the family's
+// functor is built once (per region, by the source) and called unchanged,
+// so a mixed batch computes exactly what single-family batches compute.
+template <int N>
+struct MixedGenz {
+  int family;
+  union {
+    Gaussian<N> g;
+    Oscillatory<N> o;
+    CornerPeak<N> c;
+    ProductPeak<N> p;
+    Continuous<N> ct;
+    Discontinuous<N> d;
+  } f;
+  __host__ __device__ static MixedGenz make(const GenzParams& q, int family) {
+    MixedGenz m;
+    m.family = family;
+    switch (family) {
+      case kGaussian: m.f.g = Gaussian<N>::load(q); break;
+      case kOscillatory: m.f.o = Oscillatory<N>::load(q); break;
+      case kCornerPeak: m.f.c = CornerPeak<N>::load(q); break;
+      case kProductPeak: m.f.p = ProductPeak<N>::load(q); break;
+      case kContinuous: m.f.ct = Continuous<N>::load(q); break;
+      case kDiscontinuous: m.f.d = Discontinuous<N>::load(q); break;
+      default: break;
+    }
+    return m;
+  }
+  __device__ __forceinline__ double operator()(const double* x) const {
+    switch (family) {
+      case kGaussian: return f.g(x);
+      case kOscillatory: return f.o(x);
+      case kCornerPeak: return f.c(x);
+      case kProductPeak: return f.p(x);
+      case kContinuous: return f.ct(x);
+      case kDiscontinuous: return f.d(x);
+      default: return CosSum<N>()(x);
+    }
+  }
+};
+
 }  // namespace cubature

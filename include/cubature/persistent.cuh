@@ -225,6 +225,13 @@ __device__ __forceinline__ double call_point(const F& f, const double* x, int p)
   return call_point_(f, x, p, 0);
 }
 
+// Two rule points in flight per thread, except for functors that carry
+// several families' code (the unrolled loop would not fit the registers).
+template <class F>
+constexpr bool kTwoPointsInFlight = true;
+template <int M>
+constexpr bool kTwoPointsInFlight<MixedGenz<M>> = false;
+
 template <int N>
 struct GroupSmem {
   PointTable<N> pt;
@@ -259,8 +266,8 @@ __device__ __forceinline__ RegionResult eval_region_group(const F& f, const doub
   // Branch-free body, two points in flight per thread.  A thread's points
   // of one set are consecutive, so adding into S[set] directly gives the
   // same sums as a running sum flushed at set changes.
-#pragma unroll 2
-  for (int p = active ? t : PointTable<N>::kPoints; p < PointTable<N>::kPoints; p += G) {
+  const int p0 = active ? t : PointTable<N>::kPoints;
+  auto point = [&](int p) {
     const uint2 e = sm.pt.ent[p];
     double x[N];
 #pragma unroll
@@ -269,6 +276,13 @@ __device__ __forceinline__ RegionResult eval_region_group(const F& f, const doub
     if (p <= 4 * N) sm.fstage[g][p] = fx;
 #pragma unroll
     for (int k = 0; k < kNumSets; ++k) S[k] += (e.y == (unsigned)k) ? fx : 0.0;
+  };
+  if constexpr (kTwoPointsInFlight<F>) {
+#pragma unroll 2
+    for (int p = p0; p < PointTable<N>::kPoints; p += G) point(p);
+  } else {
+#pragma unroll 1
+    for (int p = p0; p < PointTable<N>::kPoints; p += G) point(p);
   }
 #pragma unroll
   for (int k = 0; k < kNumSets; ++k) {

@@ -181,6 +181,7 @@ void cub_destroy(cub_ctx* ctx) {
   delete ctx->ws;
   if (ctx->d_params) cudaFree(ctx->d_params);
   if (ctx->d_aux) cudaFree(ctx->d_aux);
+  if (ctx->d_fams) cudaFree(ctx->d_fams);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
 }
@@ -231,6 +232,9 @@ void cub_ctx_release(cub_ctx* ctx) {
   if (ctx->d_aux) cudaFree(ctx->d_aux);
   ctx->d_aux = nullptr;
   ctx->aux_cap = 0;
+  if (ctx->d_fams) cudaFree(ctx->d_fams);
+  ctx->d_fams = nullptr;
+  ctx->fams_cap = 0;
 }
 
 void cub_ctx_reset_stats(cub_ctx* ctx) {
@@ -534,4 +538,83 @@ int cub_autotune_batch(cub_ctx* ctx, int family, int ndim, int count,
   *best = cands[bi];
   if (best_ms) *best_ms = bt;
   return 0;
+}
+
+int cub_integrate_mixed_batch(cub_ctx* ctx, int ndim, int count, const int* families,
+                              const cub_genz_params* params, const double* epsrel,
+                              const double* epsabs, double epsrel0, double epsabs0,
+                              const cub_options* opt, cub_result* out) {
+  if (!ctx || !families || !params || !out || count <= 0) {
+    set_error("invalid argument");
+    return CUB_ERR_INVALID;
+  }
+  if (!check_ndim(ndim)) return CUB_ERR_INVALID;
+  for (int k = 0; k < count; ++k)
+    if (!check_family(families[k])) return CUB_ERR_INVALID;
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+  std::vector<double> er(count), ea(count);
+  for (int k = 0; k < count; ++k) {
+    er[k] = epsrel ? epsrel[k] : epsrel0;
+    ea[k] = epsabs ? epsabs[k] : epsabs0;
+    if (!(er[k] >= 0) || !(ea[k] >= 0)) {
+      set_error("epsrel/epsabs must be >= 0");
+      return CUB_ERR_INVALID;
+    }
+  }
+  if (count > ctx->params_cap) {
+    if (ctx->d_params) cudaFree(ctx->d_params);
+    ctx->d_params = nullptr;
+    ctx->params_cap = 0;
+    if ((e = cudaMalloc(&ctx->d_params, sizeof(GenzParams) * count)) != cudaSuccess)
+      return cuda_fail(e, "cudaMalloc(params)");
+    ctx->params_cap = count;
+  }
+  if (count > ctx->fams_cap) {
+    if (ctx->d_fams) cudaFree(ctx->d_fams);
+    ctx->d_fams = nullptr;
+    ctx->fams_cap = 0;
+    if ((e = cudaMalloc(&ctx->d_fams, sizeof(int) * count)) != cudaSuccess)
+      return cuda_fail(e, "cudaMalloc(families)");
+    ctx->fams_cap = count;
+  }
+  Options o = to_options(opt);
+  if (o.max_slots <= 0) o.max_slots = ctx->ws->auto_slots(ndim, o.policy);
+  const GenzParams* h = reinterpret_cast<const GenzParams*>(params);
+  std::vector<GenzParams> hp;
+  std::vector<int> hf;
+  std::vector<double> ger, gea;
+  std::vector<Result> res;
+  const int rc = grouped_batch(count, o, [&](const std::vector<int>& idx, Result* gout) {
+    const int gn = (int)idx.size();
+    hp.resize(gn);
+    hf.resize(gn);
+    ger.resize(gn);
+    gea.resize(gn);
+    for (int j = 0; j < gn; ++j) {
+      hp[j] = h[idx[j]];
+      hf[j] = families[idx[j]];
+      ger[j] = er[idx[j]];
+      gea[j] = ea[idx[j]];
+    }
+    if (cudaMemcpyAsync(ctx->d_params, hp.data(), sizeof(GenzParams) * gn,
+                        cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess ||
+        cudaMemcpyAsync(ctx->d_fams, hf.data(), sizeof(int) * gn, cudaMemcpyHostToDevice,
+                        ctx->stream) != cudaSuccess)
+      return (int)kErrCuda;
+    ctx->ws->stats().h2d_bytes += (long long)((sizeof(GenzParams) + sizeof(int)) * gn);
+    switch (ndim) {
+      case 2: return run_mixed_dim_2(ctx, gn, ctx->d_params, ctx->d_fams, ger.data(), gea.data(), o, gout);
+      case 3: return run_mixed_dim_3(ctx, gn, ctx->d_params, ctx->d_fams, ger.data(), gea.data(), o, gout);
+      case 4: return run_mixed_dim_4(ctx, gn, ctx->d_params, ctx->d_fams, ger.data(), gea.data(), o, gout);
+      case 5: return run_mixed_dim_5(ctx, gn, ctx->d_params, ctx->d_fams, ger.data(), gea.data(), o, gout);
+      case 6: return run_mixed_dim_6(ctx, gn, ctx->d_params, ctx->d_fams, ger.data(), gea.data(), o, gout);
+      case 7: return run_mixed_dim_7(ctx, gn, ctx->d_params, ctx->d_fams, ger.data(), gea.data(), o, gout);
+      case 8: return run_mixed_dim_8(ctx, gn, ctx->d_params, ctx->d_fams, ger.data(), gea.data(), o, gout);
+    }
+    return (int)kErrInvalid;
+  }, res);
+  if (rc != kOk && rc != kErrCapacity) return engine_status(ctx, rc);
+  for (int k = 0; k < count; ++k) result_to_c(res[k], &out[k]);
+  return engine_status(ctx, rc);
 }

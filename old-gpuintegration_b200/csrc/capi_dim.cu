@@ -51,6 +51,13 @@ int rule_family(const GenzParams& p, long long n, const double* lo, const double
 
 }  // namespace
 
+int CUB_CAT(run_mixed_dim_, CUB_DIM)(cub_ctx* ctx, int count, const GenzParams* d_params,
+                                     const int* d_fams, const double* epsrel,
+                                     const double* epsabs, const Options& opt, Result* out) {
+  detail::MixedSource<N> src{d_params, d_fams};
+  return run_batch<N>(*ctx->ws, src, count, epsrel, epsabs, opt, out, ctx->stream);
+}
+
 int CUB_CAT(run_dim_, CUB_DIM)(cub_ctx* ctx, int family, int count, const GenzParams* h_params,
                                const GenzParams* d_params, const double* epsrel,
                                const double* epsabs, const Options& opt, Result* out,

@@ -18,6 +18,8 @@ struct cub_ctx {
   int params_cap = 0;
   double* d_aux = nullptr;  // per-integral scalars of the table integrands
   int aux_cap = 0;
+  int* d_fams = nullptr;  // per-integral families of mixed batches
+  int fams_cap = 0;
 };
 
 namespace cubature {
@@ -37,6 +39,9 @@ Options to_options(const cub_options* opt);
   int run_dim_##N(cub_ctx* ctx, int family, int count, const GenzParams* h_params,             \
                   const GenzParams* d_params, const double* epsrel, const double* epsabs,      \
                   const Options& opt, Result* out, const double* h_box);                       \
+  int run_mixed_dim_##N(cub_ctx* ctx, int count, const GenzParams* d_params, const int* d_fams,  \
+                        const double* epsrel, const double* epsabs, const Options& opt,         \
+                        Result* out);                                                           \
   int rule_eval_dim_##N(int family, const GenzParams& p, long long n, const double* lo,        \
                         const double* len, long long ld, double epsrel, double epsabs,         \
                         double* avg, double* err, int* axis, int* active, cudaStream_t s);     \

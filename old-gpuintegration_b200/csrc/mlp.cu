@@ -757,7 +757,7 @@ int cv_run(cub_ctx* ctx, int count, const GenzParams* h, double epsrel, double e
   std::vector<Result> coarse(count), res(count);
   double t0 = now_ms();
 
-  // 1. coarse plain run: the judge and the scale of the tolerances
+  // 1. coarse plain run: the check of the result and the scale of the tolerances
   GenzParams* d_par = nullptr;
   if (cudaMalloc(&d_par, sizeof(GenzParams) * count) != cudaSuccess)
     return cuda_error(cudaErrorMemoryAllocation, "params");
@@ -874,7 +874,7 @@ int cv_run(cub_ctx* ctx, int count, const GenzParams* h, double epsrel, double e
       cv.status = (rr.status || rg.status) ? 1 : 0;
       cv.iterations = rr.iterations + rg.iterations;
       cv.state = kStateDone;
-      // the plain coarse run judges the result
+      // the plain coarse run checks the result
       const bool agrees = std::fabs(cv.value - coarse[k].value) <=
                           3.0 * (coarse[k].error + cv.error) + 1e-300;
       if (cv.status != 0 || !agrees) {

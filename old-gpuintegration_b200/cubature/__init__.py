@@ -128,6 +128,7 @@ EXPORTS = (
     "cub_integrate_table7_batch", "cub_mlp_gemm_bf16", "cub_mlp_create", "cub_mlp_destroy",
     "cub_mlp_set_data", "cub_mlp_params", "cub_mlp_grad", "cub_mlp_train", "cub_mlp_eval",
     "cub_cv_default_options", "cub_cv_integrate_batch", "cub_autotune_batch",
+    "cub_integrate_mixed_batch",
 )
 
 _lib = None
@@ -184,6 +185,9 @@ def load_library(path: str | Path | None = None):
     L.cub_autotune_batch.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.POINTER(GenzParams),
                                      C.c_double, C.c_double, C.c_int, C.POINTER(COptions),
                                      C.POINTER(COptions), C.POINTER(C.c_double)]
+    L.cub_integrate_mixed_batch.argtypes = [vp, C.c_int, C.c_int, ip, C.POINTER(GenzParams), dp,
+                                            dp, C.c_double, C.c_double, C.POINTER(COptions),
+                                            C.POINTER(CResult)]
     L.cub_ctx_stream.argtypes = [vp]
     L.cub_ctx_stream.restype = vp
     L.cub_ctx_stats.argtypes = [vp, C.POINTER(CStats)]
@@ -474,6 +478,24 @@ class Context:
                                             epsabs, sample, C.byref(opts) if opts else None,
                                             C.byref(best), C.byref(ms)))
         return best, ms.value
+
+    def integrate_mixed(self, integrands: Sequence[Integrand], epsrel: float, epsabs: float,
+                        opts: COptions | None = None) -> list[Result]:
+        """Integrands of one dimension and any families in one call
+        (cub_integrate_mixed_batch)."""
+        n = len(integrands)
+        ndim = integrands[0].ndim
+        if any(f.ndim != ndim for f in integrands):
+            raise ValueError("a mixed batch needs one dimension")
+        fams = (C.c_int * n)(*[family_id(f.family) for f in integrands])
+        arr = (GenzParams * n)(*[f.params() for f in integrands])
+        out = (CResult * n)()
+        rc = self._lib.cub_integrate_mixed_batch(self._h, ndim, n, fams, arr, None, None,
+                                                 float(epsrel), float(epsabs),
+                                                 C.byref(opts) if opts else None, out)
+        if rc < 0 and rc != ERR_CAPACITY:
+            raise CubatureError(rc, last_error())
+        return [Result.from_c(out[i]) for i in range(n)]
 
 def spline_second_derivatives(xs, ys):
     """Natural cubic spline second derivatives (host), for device splines."""

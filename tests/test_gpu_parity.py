@@ -518,3 +518,26 @@ def _peak_params_np(n, count, seed):
     rng = np.random.default_rng(seed)
     return [(np.exp(rng.uniform(0, np.log(20), n)), rng.uniform(0.1, 0.9, n))
             for _ in range(count)]
+
+
+def test_mixed_batch_matches_single_family(cub, ctx):
+    """Integrands of different families in one call give the answers of
+    separate calls (same functors; parameters read from memory may change
+    FMA contraction in the last bit)."""
+    cases = [("oscillatory", 8, 1.1, 0.3), ("corner_peak", 8, 0.5, 0.0)]
+    fs = [cub.Integrand(f, n, a, u) for f, n, a, u in cases]
+    mixed = ctx.integrate_mixed(fs, 1e-6, 1e-12)
+    for f, m in zip(fs, mixed):
+        s = ctx.integrate(f, 1e-6, 1e-12)
+        assert m.status == s.status and m.nregions == s.nregions
+        assert abs(m.integral - s.integral) <= 1e-13 * abs(s.integral)
+    fams = [("gaussian", [4.0, 6.0, 5.0, 3.0], [0.3, 0.5, 0.6, 0.4]),
+            ("product_peak", [8.0, 12.0, 6.0, 10.0], [0.3, 0.6, 0.5, 0.4]),
+            ("continuous", [3.0, 4.0, 2.0, 5.0], [0.4, 0.6, 0.5, 0.5]),
+            ("cossum", 1.0, 0.0)]
+    fs = [cub.Integrand(f, 4, a, u) for f, a, u in fams]
+    mixed = ctx.integrate_mixed(fs, 1e-6, 1e-12)
+    for f, m in zip(fs, mixed):
+        s = ctx.integrate_batch(f.family, 4, [f.params()], 1e-6, 1e-12)[0]
+        assert m.status == s.status and m.nregions == s.nregions
+        assert abs(m.integral - s.integral) <= 1e-13 * abs(s.integral) + 1e-15
