@@ -917,6 +917,31 @@ __global__ void __launch_bounds__(256, 2) k_persistent(Src src, RuleTables T, Pe
   for (int it = 0;; ++it) {
     if (tracer) trace_mark(ctl, it, 0);
     const int parity = it & 1;
+    const bool lazy = it > 0;
+    if (lazy) {
+      // Stage the lookups of the lazy split while the iteration state is
+      // read: they depend only on the parent list and the integral states,
+      // both complete at the grid barrier.  materialize and handoff do not
+      // touch the staged copy.
+      const int* pexcl = p.excl[parity ^ 1];
+      const unsigned* pmask = p.cmask[parity ^ 1];
+      const int pnc = (int)(prev_n / 32);
+      for (int q = threadIdx.x; q < pnc; q += blockDim.x) {
+        sg.excl[q] = pexcl[q];
+        sg.mask[q] = pmask[q];
+      }
+      if (small) {
+        for (int q = threadIdx.x; q < p.base.nint; q += blockDim.x) {
+          const IntegralState& is = p.base.ist[q];
+          sg.seg_start[q] = is.seg_start;
+          sg.seg_count[q] = is.seg_count;
+          sg.par_start[q] = is.par_start;
+          sg.par_count[q] = is.par_count;
+          sg.epsrel[q] = is.epsrel;
+          sg.epsabs[q] = is.epsabs;
+        }
+      }
+    }
     {
       volatile IterState* v = &ctl->it[parity];
       st.n = v->n;
@@ -925,7 +950,6 @@ __global__ void __launch_bounds__(256, 2) k_persistent(Src src, RuleTables T, Pe
       st.overflow = v->overflow;
       st.handoff = v->handoff;
     }
-    const bool lazy = it > 0;
     const int mode = lazy ? kSlotLazy : (p.init ? kSlotGrid : kSlotStored);
     EngineArgs a = p.base;
     a.lo = p.lo[cur];
@@ -961,34 +985,14 @@ __global__ void __launch_bounds__(256, 2) k_persistent(Src src, RuleTables T, Pe
       break;
     }
     if (lazy && st.handoff) detail::handoff<N>(a, P, prid, prev_n, g_it);
-    if (lazy && blockIdx.x < st.n) {
-      // stage the lookups of the lazy split (blocks with slots only)
-      const int pnc = (int)(prev_n / 32);
-      for (int q = threadIdx.x; q < pnc; q += blockDim.x) {
-        sg.excl[q] = P.excl[q];
-        sg.mask[q] = P.mask[q];
-      }
-      if (small) {
-        for (int q = threadIdx.x; q < a.nint; q += blockDim.x) {
-          const IntegralState& is = a.ist[q];
-          sg.seg_start[q] = is.seg_start;
-          sg.seg_count[q] = is.seg_count;
-          sg.par_start[q] = is.par_start;
-          sg.par_count[q] = is.par_count;
-          sg.epsrel[q] = is.epsrel;
-          sg.epsabs[q] = is.epsabs;
-        }
-      } else {
-        for (int q = threadIdx.x; q < st.n / 32; q += blockDim.x) sg.cint[q] = p.chunk_int[q];
-      }
-      __syncthreads();
-    }
+    if (lazy && !small)
+      for (int q = threadIdx.x; q < st.n / 32; q += blockDim.x) sg.cint[q] = p.chunk_int[q];
     IterState* next = &ctl->it[parity ^ 1];
     // The chain after a chunk runs out of line (one warp per chunk, cold
     // code shared by all group sizes); it reads the arguments from a
     // shared-memory copy so that the kernel's own copy stays in registers.
     if (threadIdx.x == 0) sargs = a;
-    __syncthreads();
+    __syncthreads();  // also publishes the staged lookups
 
     // smallest R (regions per block) that covers the list in one pass
     const long long per_block = (st.n + gridDim.x - 1) / gridDim.x;
