@@ -86,11 +86,14 @@ __device__ __forceinline__ void red_release_add(unsigned* p, unsigned v) {
 // Grid-wide barrier on a monotonic arrival counter: the b-th barrier of a
 // launch (b = 1, 2, ...) waits for b * gridDim.x arrivals.  Bounded wait;
 // returns false once any block gave up waiting (all blocks then return).
+// Ordering needs no separate fences: the block's writes precede thread 0's
+// gpu-scope release through the CTA barrier, the release and acquire
+// operations are cumulative, and the closing CTA barrier orders the
+// block's later reads after thread 0's acquire.
 __device__ __forceinline__ bool grid_barrier(Control* ctl, unsigned target) {
   __shared__ int ok;
   __syncthreads();
   if (threadIdx.x == 0) {
-    __threadfence();
     red_release_add(&ctl->bar_count, 1u);
     long long spins = 0;
     int good = 1;
@@ -102,7 +105,6 @@ __device__ __forceinline__ bool grid_barrier(Control* ctl, unsigned target) {
       }
       __nanosleep(32);
     }
-    __threadfence();
     ok = good && *(volatile int*)&ctl->timeout == 0;
   }
   __syncthreads();
@@ -709,7 +711,7 @@ static __device__ __noinline__ void after_chunk_warp(const EngineArgs& a, long l
       trace_mark(a.ctl, it, 5);
     }
     decide_scan_small(a, st, next, lane, g_next, it);
-    __threadfence();
+    // the next list becomes visible through the grid barrier's release
     if (lane == 0) trace_mark(a.ctl, it, 1);
     return;
   }
@@ -732,7 +734,7 @@ static __device__ __noinline__ void after_chunk_warp(const EngineArgs& a, long l
   __syncwarp();
   if (lane == 0) a.ctl->done_cnt = 0;
   scan_shift_warp(a, st.n_left, next, chunk_int, lane, g_next);
-  __threadfence();
+  // the next list becomes visible through the grid barrier's release
   if (lane == 0) trace_mark(a.ctl, it, 1);
 }
 
