@@ -483,6 +483,33 @@ def main() -> int:
         single_cmp = {"value": len(items) * len(ms) / (sum(ms) / 1e3), "unit": "integrals/s",
                       "ms_per_step": sum(ms) / len(ms),
                       "call": "cub_integrate_mixed_batch, all integrands in one call"}
+    graph_cmp = None
+    if "items" in workload:
+        # the same integrals as one replayed CUDA graph (cub_graph_launch:
+        # one graph launch and one wait per step), timed the same way
+        g = ctx.graph([(f.family, f.ndim, 1) for f in items], opts)
+        for _ in range(3):
+            g.launch(items, workload["epsrel"], workload["epsabs"])
+        ms, wms = [], []
+        for _ in range(max(3, args.steps)):
+            flush.zero_()
+            torch.cuda.synchronize()
+            s0 = torch.cuda.Event(enable_timing=True)
+            s1 = torch.cuda.Event(enable_timing=True)
+            s0.record(stream)
+            t0 = time.perf_counter()
+            g.launch(items, workload["epsrel"], workload["epsabs"])
+            t1 = time.perf_counter()
+            s1.record(stream)
+            torch.cuda.synchronize()
+            ms.append(s0.elapsed_time(s1))
+            wms.append((t1 - t0) * 1e3)
+        replays, reruns = g.info()
+        g.close()
+        graph_cmp = {"value": len(items) * len(ms) / (sum(ms) / 1e3), "unit": "integrals/s",
+                     "e2e": len(items) * len(wms) / (sum(wms) / 1e3),
+                     "ms_per_step": sum(ms) / len(ms), "replays": replays, "reruns": reruns,
+                     "call": "cub_graph_launch, every integrand in one replayed CUDA graph"}
     if "cv" in workload:
         # the plain method on the same integrands, same tolerance, one pass
         torch.cuda.synchronize()
@@ -580,6 +607,8 @@ def main() -> int:
         if single_cmp is not None:
             line["config"]["call"] = "cub_integrate, one call per integrand"
             line["mixed_call"] = single_cmp
+        if graph_cmp is not None:
+            line["graph_call"] = graph_cmp
         print(json.dumps(line), flush=True)
     ctx.close()
     if pg:

@@ -218,6 +218,41 @@ int cub_autotune_batch(cub_ctx* ctx, int family, int ndim, int count,
                        const cub_genz_params* params, double epsrel, double epsabs, int sample,
                        const cub_options* opt, cub_options* best, double* best_ms);
 
+/* ---- replayable batches (CUDA graph) ---------------------------------- */
+
+/* Repeated integrations of the same shape -- the same families,
+ * dimensions and counts, new parameters and tolerances each call -- as one
+ * captured CUDA graph.  Entry i is a batch of counts[i] integrals of
+ * families[i] in ndims[i] dimensions over the unit cube.  The graph records
+ * per entry the parameter and state uploads, one cooperative persistent
+ * launch (initial grid and every breadth-first iteration while the list
+ * stays within the persistent kernel's limit) and the state download; each
+ * entry has its own region lists, so the recorded pointers never change.
+ * The initial grid of each entry must fit the persistent limit
+ * (CUB_ERR_UNSUPPORTED otherwise).  No counterpart in the reference: its
+ * integrate (GPUquad.h:611-727) drives every iteration from the host,
+ * with device-to-host copies in between (GPUKernelquad.cu:565-598). */
+typedef struct cub_graph cub_graph;
+
+int cub_graph_create(cub_ctx* ctx, int nentries, const int* families, const int* ndims,
+                     const int* counts, const cub_options* opt, cub_graph** out);
+
+/* One replay: params, epsrel, epsabs and out hold every entry's integrals
+ * in entry order (sum of counts).  Parameters and starting states are
+ * written to pinned buffers, the graph is launched on the context's stream
+ * and waited for once.  An entry that the launch did not finish (its list
+ * outgrew the persistent limit, or boxes went to phase 2) is integrated
+ * again by cub_integrate_batch, so every result equals that call's.
+ * Returns 0, CUB_ERR_CAPACITY (as cub_integrate_batch) or an error. */
+int cub_graph_launch(cub_graph* g, const cub_genz_params* params, const double* epsrel,
+                     const double* epsabs, cub_result* out);
+
+/* Replays so far, and entries that needed cub_integrate_batch after one. */
+int cub_graph_info(const cub_graph* g, long long* replays, long long* reruns);
+
+/* Free the graph and its buffers; call it before cub_destroy of its context. */
+void cub_graph_destroy(cub_graph* g);
+
 /* ---- integrands on device tables ------------------------------------- */
 
 /* Rectilinear 2-D table in device memory, row-major zs[i * ny + j] at

@@ -144,6 +144,7 @@ class Workspace {
   int device() const { return device_; }
   bool timing = false;  // record CUDA events around the rule, persistent and phase-2 kernels
   const std::string& error() const { return err_; }
+  void set_error(const std::string& m) { err_ = m; }
   Stats& stats() { return stats_; }
 
   // Buffers (valid after the reserve_* calls).
@@ -460,6 +461,158 @@ inline void launch_eval(const Src& src, const RuleTables& T, const EngineArgs& a
   k_eval<N, K, Src><<<(unsigned)blocks, 256, 0, s>>>(src, T, a);
 }
 
+namespace detail {
+
+// Host copy of a batch's starting point: integral k owns the k-th padded
+// segment of the initial grid.  Fills the pinned states behind
+// ws.ctl_host_ and returns the control block the first launch starts from.
+inline Control initial_states(Workspace& ws, int nint, const double* epsrel,
+                              const double* epsabs, int per, int padded, long long n0) {
+  IntegralState* h = ws.ist_host_;
+  for (int k = 0; k < nint; ++k) {
+    IntegralState& is = h[k];
+    std::memset(&is, 0, sizeof(is));
+    is.epsrel = epsrel[k];
+    is.epsabs = epsabs[k];
+    is.state = kStateRunning;
+    is.seg_start = k * padded;
+    is.seg_count = per;
+  }
+  Control c0;
+  std::memset(&c0, 0, sizeof(c0));
+  c0.host.n = (int)n0;
+  c0.host.n_running = nint;
+  return c0;
+}
+
+// Results from the final integral states.
+inline void state_results(const IntegralState* h, int nint, Result* out) {
+  for (int k = 0; k < nint; ++k) {
+    const IntegralState& is = h[k];
+    Result& r = out[k];
+    r.nregions = is.nregions;
+    r.neval = is.neval;
+    r.iterations = is.iters;
+    r.state = is.state;
+    r.pad = 0;
+    if (is.state == kStateRunning || is.state == kStateCapacity) {
+      // stopped early: report the last full estimate, not converged
+      r.value = is.last_value;
+      r.error = is.last_error;
+      r.status = is.last_error <= detail::max_err(is.last_value, is.epsrel, is.epsabs) ? 0 : 1;
+    } else {
+      r.value = is.value;
+      r.error = is.error;
+      r.status = is.status;
+    }
+  }
+}
+
+// Blocks of a cooperative k_persistent<N, Src> launch on the workspace's
+// device (queried once per device and instantiation); 0 when the device
+// has no cooperative launch.
+template <int N, class Src>
+int persistent_blocks(const Workspace& ws, int sms) {
+  static int per_sm_cache[64];
+  static bool cached[64];
+  const int dev = ws.device() & 63;
+  if (!cached[dev]) {
+    int per_sm = 0, coop = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_persistent<N, Src>, 256, 0);
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, ws.device());
+    per_sm_cache[dev] = coop ? per_sm : 0;
+    cached[dev] = true;
+  }
+  return per_sm_cache[dev] > 0 ? per_sm_cache[dev] * sms : 0;
+}
+
+// Longest list a persistent launch keeps iterating on.
+inline int persistent_limit(const Options& opt, int pblocks) {
+  return std::min(opt.persistent_max_n > 0 ? opt.persistent_max_n : pblocks * 8 * 8,
+                  32 * kStageChunks);
+}
+
+// Engine arguments of a batch; bind_lists points them at list `cur`.
+inline EngineArgs engine_args(const Workspace& ws, int nint, const Options& opt, int npoints) {
+  EngineArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.ist = ws.ist;
+  a.nint = nint;
+  a.ctl = ws.ctl;
+  a.policy = opt.policy;
+  a.phase1_cap = opt.policy == kPolicyReference ? opt.phase1_cap : 0;
+  a.max_iters = opt.max_iters;
+  a.npoints = npoints;
+  return a;
+}
+
+inline void bind_lists(const Workspace& ws, EngineArgs& a, int cur, long long n) {
+  a.lo = ws.lo[cur];
+  a.len = ws.len[cur];
+  a.rid = ws.rid[cur];
+  a.n = (int)n;
+  a.cap = ws.cap();
+  a.avg = ws.avg;
+  a.err = ws.err;
+  a.axis = ws.axis;
+  a.active = ws.active;
+  a.part = ws.part;
+  a.chunk_excl = ws.chunk_excl;
+  a.chunk_cnt = ws.chunk_cnt;
+  a.int_cnt = ws.int_cnt;
+  a.nlo = ws.lo[cur ^ 1];
+  a.nlen = ws.len[cur ^ 1];
+  a.nrid = ws.rid[cur ^ 1];
+  a.ncap = ws.cap();
+  a.left_lo = ws.left_lo;
+  a.left_len = ws.left_len;
+  a.left_rid = ws.left_rid;
+  a.left_cap = ws.left_cap();
+}
+
+// Arguments of a persistent launch over the lists bound in `a`.
+inline PersistArgs persist_args(const Workspace& ws, const EngineArgs& a, const Options& opt,
+                                int iter_base, int pmax, bool init, int dv, int per, int padded,
+                                const double* d_box) {
+  PersistArgs p;
+  p.base = a;
+  const long long nchunk = ws.cap() / 32 + 1;
+  for (int b = 0; b < 2; ++b) {
+    p.lo[b] = ws.lo[b];
+    p.len[b] = ws.len[b];
+    p.rid[b] = ws.rid[b];
+    p.cmask[b] = ws.cmask + b * nchunk;
+  }
+  p.axis[0] = ws.axis;
+  p.axis[1] = ws.axis_alt;
+  p.excl[0] = ws.chunk_excl;
+  p.excl[1] = ws.excl_alt;
+  p.chunk_int = ws.chunk_int;
+  p.iter_base = iter_base;
+  p.max_n = pmax;
+  p.max_r = opt.persistent_max_r > 0 ? opt.persistent_max_r : 8;
+  p.init = init ? 1 : 0;
+  p.divisions = dv;
+  p.per_integral = per;
+  p.padded = padded;
+  p.box = d_box;
+  return p;
+}
+
+// Pinned control block for a persistent launch starting from `hs`.
+inline void persistent_control(Workspace& ws, const IterState& hs, int cur) {
+  ws.ctl_host_->host = hs;
+  ws.ctl_host_->it[0] = hs;
+  ws.ctl_host_->cur = cur;
+  ws.ctl_host_->done_cnt = 0;
+  ws.ctl_host_->bar_count = 0;
+  ws.ctl_host_->timeout = 0;
+  ws.ctl_host_->exit_reason = 0;
+  std::memset(ws.ctl_host_->trace, 0, sizeof(ws.ctl_host_->trace));
+}
+
+}  // namespace detail
+
 // Rule evaluation step of the multi-launch driver when the caller supplies
 // its own (NoHook: the engine's k_eval).  A hook's eval(args, n, stream)
 // evaluates the n slots of the current list into args.avg/err/axis/active
@@ -497,19 +650,7 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
 
   // integral states
   IntegralState* h = ws.ist_host_;
-  for (int k = 0; k < nint; ++k) {
-    IntegralState& is = h[k];
-    std::memset(&is, 0, sizeof(is));
-    is.epsrel = epsrel[k];
-    is.epsabs = epsabs[k];
-    is.state = kStateRunning;
-    is.seg_start = k * padded;
-    is.seg_count = per;
-  }
-  Control c0;
-  std::memset(&c0, 0, sizeof(c0));
-  c0.host.n = (int)n_cur;
-  c0.host.n_running = nint;
+  Control c0 = detail::initial_states(ws, nint, epsrel, epsabs, per, padded, n_cur);
   *ws.ctl_host_ = c0;
   // The control block and the states go to the device with the first
   // launch (one copy); the initial grid is written by k_init_grid or, when
@@ -527,57 +668,14 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
   }
 
   int cur = 0;
-  EngineArgs a;
-  std::memset(&a, 0, sizeof(a));
-  a.ist = ws.ist;
-  a.nint = nint;
-  a.ctl = ws.ctl;
-  a.policy = opt.policy;
-  a.phase1_cap = opt.policy == kPolicyReference ? opt.phase1_cap : 0;
-  a.max_iters = opt.max_iters;
-  a.npoints = T.npoints;
-  auto bind = [&](long long n) {
-    a.lo = ws.lo[cur];
-    a.len = ws.len[cur];
-    a.rid = ws.rid[cur];
-    a.n = (int)n;
-    a.cap = ws.cap();
-    a.avg = ws.avg;
-    a.err = ws.err;
-    a.axis = ws.axis;
-    a.active = ws.active;
-    a.part = ws.part;
-    a.chunk_excl = ws.chunk_excl;
-    a.chunk_cnt = ws.chunk_cnt;
-    a.int_cnt = ws.int_cnt;
-    a.nlo = ws.lo[cur ^ 1];
-    a.nlen = ws.len[cur ^ 1];
-    a.nrid = ws.rid[cur ^ 1];
-    a.ncap = ws.cap();
-    a.left_lo = ws.left_lo;
-    a.left_len = ws.left_len;
-    a.left_rid = ws.left_rid;
-    a.left_cap = ws.left_cap();
-  };
+  EngineArgs a = detail::engine_args(ws, nint, opt, T.npoints);
+  auto bind = [&](long long n) { detail::bind_lists(ws, a, cur, n); };
   bind(n_cur);
 
   // persistent kernel geometry (queried once per device and instantiation)
-  int pblocks = 0;
-  if (opt.persistent && !Hook::kActive) {
-    static int per_sm_cache[64];
-    static bool cached[64];
-    const int dev = ws.device() & 63;
-    if (!cached[dev]) {
-      int per_sm = 0, coop = 0;
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_persistent<N, Src>, 256, 0);
-      cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, ws.device());
-      per_sm_cache[dev] = coop ? per_sm : 0;
-      cached[dev] = true;
-    }
-    if (per_sm_cache[dev] > 0) pblocks = per_sm_cache[dev] * sms;
-  }
-  const int pmax = std::min(opt.persistent_max_n > 0 ? opt.persistent_max_n : pblocks * 8 * 8,
-                            32 * kStageChunks);
+  const int pblocks =
+      opt.persistent && !Hook::kActive ? detail::persistent_blocks<N, Src>(ws, sms) : 0;
+  const int pmax = detail::persistent_limit(opt, pblocks);
 
   IterState hs = c0.host;
   long long n_left = 0;
@@ -601,41 +699,14 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
 
     if (pblocks > 0 && n_cur <= pmax) {
       // a stretch of iterations in one persistent launch
-      ws.ctl_host_->host = hs;
-      ws.ctl_host_->it[0] = hs;
-      ws.ctl_host_->cur = cur;
-      ws.ctl_host_->done_cnt = 0;
-      ws.ctl_host_->bar_count = 0;
-      ws.ctl_host_->timeout = 0;
-      ws.ctl_host_->exit_reason = 0;
-      std::memset(ws.ctl_host_->trace, 0, sizeof(ws.ctl_host_->trace));
+      detail::persistent_control(ws, hs, cur);
       const size_t up = uploaded ? sizeof(Control) : ws.state_bytes(nint);
       if (!ws.ck(cudaMemcpyAsync(ws.ctl, ws.ctl_host_, up, cudaMemcpyHostToDevice, s)))
         return kErrCuda;
       uploaded = true;
       st.h2d_bytes += (long long)up;
-      PersistArgs p;
-      p.base = a;
-      const long long nchunk = ws.cap() / 32 + 1;
-      for (int b = 0; b < 2; ++b) {
-        p.lo[b] = ws.lo[b];
-        p.len[b] = ws.len[b];
-        p.rid[b] = ws.rid[b];
-        p.cmask[b] = ws.cmask + b * nchunk;
-      }
-      p.axis[0] = ws.axis;
-      p.axis[1] = ws.axis_alt;
-      p.excl[0] = ws.chunk_excl;
-      p.excl[1] = ws.excl_alt;
-      p.chunk_int = ws.chunk_int;
-      p.iter_base = c0.iters_done;
-      p.max_n = pmax;
-      p.max_r = opt.persistent_max_r > 0 ? opt.persistent_max_r : 8;
-      p.init = grid_pending ? 1 : 0;
-      p.divisions = dv;
-      p.per_integral = per;
-      p.padded = padded;
-      p.box = d_box;
+      PersistArgs p = detail::persist_args(ws, a, opt, c0.iters_done, pmax, grid_pending, dv,
+                                           per, padded, d_box);
       grid_pending = false;
       void* args[] = {(void*)&src, (void*)&T, (void*)&p};
       if (ws.timing) ws.ck(cudaEventRecord(ws.ev[0], s));
@@ -782,26 +853,126 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
     cudaEventElapsedTime(&ms, ws.ev[2], ws.ev[3]);
     st.ms_phase2 += ms;
   }
-  for (int k = 0; k < nint; ++k) {
-    const IntegralState& is = h[k];
-    Result& r = out[k];
-    r.nregions = is.nregions;
-    r.neval = is.neval;
-    r.iterations = is.iters;
-    r.state = is.state;
-    r.pad = 0;
-    if (is.state == kStateRunning || is.state == kStateCapacity) {
-      // stopped early: report the last full estimate, not converged
-      r.value = is.last_value;
-      r.error = is.last_error;
-      r.status = is.last_error <= detail::max_err(is.last_value, is.epsrel, is.epsabs) ? 0 : 1;
-    } else {
-      r.value = is.value;
-      r.error = is.error;
-      r.status = is.status;
-    }
-  }
+  detail::state_results(h, nint, out);
   return status;
+}
+
+// A batch prepared for replay, for instance from a CUDA graph: the stream
+// work of run_batch's first persistent launch (upload of the starting
+// states, one cooperative launch that lays out the initial grid and runs
+// every breadth-first iteration while the list stays within the persistent
+// limit, download of the states).  Every buffer is reserved by
+// replay_prepare, so the pointers in the recorded work stay valid for the
+// workspace's lifetime as long as nothing else reserves in it.
+//
+// One replay completes the batch when every integral stops inside the
+// launch (converged, or out of iterations) without phase-2 boxes;
+// replay_finish says whether it did.  The launch is the one run_batch makes
+// first, so a completed replay equals run_batch's result; otherwise the
+// caller integrates the batch with run_batch.
+struct Replay {
+  int nint = 0;
+  int pblocks = 0;
+  int per = 0, padded = 0;
+  long long n0 = 0;
+  PersistArgs p;
+};
+
+template <int N, class Src>
+int replay_prepare(Workspace& ws, int nint, const Options& opt, cudaStream_t s, Replay* r) {
+  static_assert(N >= 2 && N <= kMaxDim, "dimension out of range");
+  if (nint <= 0 || !r) return kErrInvalid;
+  const long long max_slots = opt.max_slots > 0 ? opt.max_slots : ws.auto_slots(N, opt.policy);
+  const int sms = sm_count(ws.device());
+  const int dv = grid_divisions(N);
+  int per = 1;
+  for (int d = 0; d < N; ++d) per *= dv;
+  const int padded = (per + 31) & ~31;
+  const long long n0 = (long long)nint * padded;
+  const int pblocks = opt.persistent ? detail::persistent_blocks<N, Src>(ws, sms) : 0;
+  const int pmax = detail::persistent_limit(opt, pblocks);
+  if (pblocks <= 0 || n0 > pmax) {
+    ws.set_error("replay needs the persistent kernel and an initial grid of at most " +
+                 std::to_string(pmax) + " regions");
+    return kErrUnsupported;
+  }
+  // Lists for the longest list the launch iterates on: it leaves on length
+  // (n > pmax) before the capacity test (2n + 32 nint > cap) can stop it,
+  // as in run_batch, whose first reservation is larger.  Leftover room as
+  // run_batch reserves before its first launch.
+  const long long need = 2 * n0 + 32ll * nint;
+  if (need > max_slots) return kErrCapacity;
+  if (!ws.reserve_integrals(nint, s)) return kErrCuda;
+  if (!ws.reserve_lists(N, std::min<long long>(2ll * pmax + 32ll * nint + 64, max_slots), 0, 0,
+                        s, max_slots))
+    return kErrCuda;
+  if (!ws.reserve_leftovers(N, opt.policy == kPolicyReference ? 4 * n0 + 1 : 1, 0, s))
+    return kErrCuda;
+  const RuleTables T = make_rule9_tables(N);
+  EngineArgs a = detail::engine_args(ws, nint, opt, T.npoints);
+  detail::bind_lists(ws, a, 0, n0);
+  r->nint = nint;
+  r->pblocks = pblocks;
+  r->per = per;
+  r->padded = padded;
+  r->n0 = n0;
+  r->p = detail::persist_args(ws, a, opt, 0, pmax, true, dv, per, padded, nullptr);
+  return kOk;
+}
+
+// Starting states of one replay (pinned host memory; read by the upload
+// that replay_enqueue records).
+inline void replay_states(Workspace& ws, const Replay& r, const double* epsrel,
+                          const double* epsabs) {
+  const Control c0 = detail::initial_states(ws, r.nint, epsrel, epsabs, r.per, r.padded, r.n0);
+  *ws.ctl_host_ = c0;
+  detail::persistent_control(ws, c0.host, 0);
+}
+
+// Record (or issue) the replay's stream work on s; nothing here waits for
+// the device, so the calls may be captured.
+template <int N, class Src>
+int replay_enqueue(Workspace& ws, const Src& src, const Replay& r, cudaStream_t s) {
+  static const RuleTables T = make_rule9_tables(N);
+  const size_t bytes = ws.state_bytes(r.nint);
+  if (!ws.ck(cudaMemcpyAsync(ws.ctl, ws.ctl_host_, bytes, cudaMemcpyHostToDevice, s)))
+    return kErrCuda;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)r.pblocks);
+  cfg.blockDim = dim3(256);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  if (!ws.ck(cudaLaunchKernelEx(&cfg, k_persistent<N, Src>, src, T, r.p))) return kErrCuda;
+  if (!ws.ck(cudaMemcpyAsync(ws.ctl_host_, ws.ctl, bytes, cudaMemcpyDeviceToHost, s)))
+    return kErrCuda;
+  return kOk;
+}
+
+// After the replay's work has completed: 1 and the results in out[0..nint)
+// when the launch finished the batch, 0 when it did not (the list outgrew
+// the persistent limit, or boxes went to phase 2), or a negative ErrorCode.
+inline int replay_finish(Workspace& ws, const Replay& r, Result* out) {
+  const Control& c = *ws.ctl_host_;
+  Stats& st = ws.stats();
+  st.launches += 1;
+  st.persistent_launches += 1;
+  st.iterations += c.iters_done;
+  st.persistent_iterations += c.iters_done;
+  st.h2d_bytes += (long long)ws.state_bytes(r.nint);
+  st.d2h_bytes += (long long)ws.state_bytes(r.nint);
+  if (c.exit_reason == kExitTimeout || c.timeout) {
+    ws.ck(cudaErrorLaunchTimeout);
+    return kErrTimeout;
+  }
+  const IterState& hs = c.host;
+  if ((hs.n_running > 0 && hs.n > 0) || hs.n_left > 0) return 0;
+  detail::state_results(ws.ist_host_, r.nint, out);
+  return 1;
 }
 
 }  // namespace cubature

@@ -55,6 +55,7 @@ def units() -> list[tuple[Path, Path, list[str]]]:
     out = [(CSRC / "capi.cu", OBJ / "capi.o", []),
            (CSRC / "noalloc.cu", OBJ / "noalloc.o", []),
            (CSRC / "capi_tables.cu", OBJ / "capi_tables.o", []),
+           (CSRC / "graph.cu", OBJ / "graph.o", []),
            (CSRC / "mlp.cu", OBJ / "mlp.o", [])]
     for n in DIMS:
         out.append((CSRC / "capi_dim.cu", OBJ / f"capi_dim{n}.o", [f"-DCUB_DIM={n}"]))

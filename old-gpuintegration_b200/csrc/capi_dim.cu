@@ -49,7 +49,49 @@ int rule_family(const GenzParams& p, long long n, const double* lo, const double
   return 0;
 }
 
+// A batch of one family for replay: its integrands read their parameters
+// from device memory, so one recording serves every call.
+template <template <int> class Fam>
+int replay_prepare_family(Workspace& ws, int count, const Options& opt, cudaStream_t s,
+                          Replay* r) {
+  return replay_prepare<N, detail::ParamSource<Fam<N>>>(ws, count, opt, s, r);
+}
+
+template <template <int> class Fam>
+int replay_enqueue_family(Workspace& ws, const GenzParams* d_params, const Replay& r,
+                          cudaStream_t s) {
+  return replay_enqueue<N>(ws, detail::ParamSource<Fam<N>>{d_params}, r, s);
+}
+
 }  // namespace
+
+int CUB_CAT(replay_prepare_dim_, CUB_DIM)(int family, Workspace& ws, int count,
+                                          const Options& opt, cudaStream_t s, Replay* r) {
+  switch (family) {
+    case kGaussian: return replay_prepare_family<Gaussian>(ws, count, opt, s, r);
+    case kOscillatory: return replay_prepare_family<Oscillatory>(ws, count, opt, s, r);
+    case kCornerPeak: return replay_prepare_family<CornerPeak>(ws, count, opt, s, r);
+    case kProductPeak: return replay_prepare_family<ProductPeak>(ws, count, opt, s, r);
+    case kContinuous: return replay_prepare_family<Continuous>(ws, count, opt, s, r);
+    case kDiscontinuous: return replay_prepare_family<Discontinuous>(ws, count, opt, s, r);
+    case kCosSum: return replay_prepare_family<CosSum>(ws, count, opt, s, r);
+  }
+  return CUB_ERR_INVALID;
+}
+
+int CUB_CAT(replay_enqueue_dim_, CUB_DIM)(int family, Workspace& ws, const GenzParams* d_params,
+                                          const Replay& r, cudaStream_t s) {
+  switch (family) {
+    case kGaussian: return replay_enqueue_family<Gaussian>(ws, d_params, r, s);
+    case kOscillatory: return replay_enqueue_family<Oscillatory>(ws, d_params, r, s);
+    case kCornerPeak: return replay_enqueue_family<CornerPeak>(ws, d_params, r, s);
+    case kProductPeak: return replay_enqueue_family<ProductPeak>(ws, d_params, r, s);
+    case kContinuous: return replay_enqueue_family<Continuous>(ws, d_params, r, s);
+    case kDiscontinuous: return replay_enqueue_family<Discontinuous>(ws, d_params, r, s);
+    case kCosSum: return replay_enqueue_family<CosSum>(ws, d_params, r, s);
+  }
+  return CUB_ERR_INVALID;
+}
 
 int CUB_CAT(run_mixed_dim_, CUB_DIM)(cub_ctx* ctx, int count, const GenzParams* d_params,
                                      const int* d_fams, const double* epsrel,

@@ -48,7 +48,11 @@ Options to_options(const cub_options* opt);
   int split_dim_##N(long long n, const double* lo, const double* len, long long ld,            \
                     const int* active, const int* axis, double* olo, double* olen,             \
                     long long old, int layout, long long* count, int* cnt, int* excl,          \
-                    cudaStream_t s);
+                    cudaStream_t s);                                                           \
+  int replay_prepare_dim_##N(int family, Workspace& ws, int count, const Options& opt,          \
+                             cudaStream_t s, Replay* r);                                        \
+  int replay_enqueue_dim_##N(int family, Workspace& ws, const GenzParams* d_params,             \
+                             const Replay& r, cudaStream_t s);
 CUB_DECLARE_DIM(2)
 CUB_DECLARE_DIM(3)
 CUB_DECLARE_DIM(4)

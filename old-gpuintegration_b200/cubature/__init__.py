@@ -128,7 +128,8 @@ EXPORTS = (
     "cub_integrate_table7_batch", "cub_mlp_gemm_bf16", "cub_mlp_create", "cub_mlp_destroy",
     "cub_mlp_set_data", "cub_mlp_params", "cub_mlp_grad", "cub_mlp_train", "cub_mlp_eval",
     "cub_cv_default_options", "cub_cv_integrate_batch", "cub_autotune_batch",
-    "cub_integrate_mixed_batch",
+    "cub_integrate_mixed_batch", "cub_graph_create", "cub_graph_launch", "cub_graph_info",
+    "cub_graph_destroy",
 )
 
 _lib = None
@@ -188,6 +189,12 @@ def load_library(path: str | Path | None = None):
     L.cub_integrate_mixed_batch.argtypes = [vp, C.c_int, C.c_int, ip, C.POINTER(GenzParams), dp,
                                             dp, C.c_double, C.c_double, C.POINTER(COptions),
                                             C.POINTER(CResult)]
+    L.cub_graph_create.argtypes = [vp, C.c_int, ip, ip, ip, C.POINTER(COptions),
+                                   C.POINTER(vp)]
+    L.cub_graph_launch.argtypes = [vp, C.POINTER(GenzParams), dp, dp, C.POINTER(CResult)]
+    L.cub_graph_info.argtypes = [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
+    L.cub_graph_destroy.argtypes = [vp]
+    L.cub_graph_destroy.restype = None
     L.cub_ctx_stream.argtypes = [vp]
     L.cub_ctx_stream.restype = vp
     L.cub_ctx_stats.argtypes = [vp, C.POINTER(CStats)]
@@ -496,6 +503,70 @@ class Context:
         if rc < 0 and rc != ERR_CAPACITY:
             raise CubatureError(rc, last_error())
         return [Result.from_c(out[i]) for i in range(n)]
+
+    def graph(self, entries: Sequence[tuple], opts: COptions | None = None) -> "Graph":
+        """A replayable graph of (family, ndim, count) batches (cub_graph_create)."""
+        return Graph(self, entries, opts)
+
+class Graph:
+    """Repeated integrations of one shape as a replayed CUDA graph
+    (cub_graph_*): entries are (family, ndim, count) batches; launch()
+    takes every entry's integrands in entry order."""
+
+    def __init__(self, ctx: "Context", entries: Sequence[tuple], opts: COptions | None = None):
+        self._lib = ctx._lib
+        self._ctx = ctx  # the graph runs on the context's stream and device
+        self.entries = [(f, int(n), int(c)) for f, n, c in entries]
+        m = len(self.entries)
+        fams = (C.c_int * m)(*[family_id(f) for f, _, _ in self.entries])
+        dims = (C.c_int * m)(*[n for _, n, _ in self.entries])
+        cnts = (C.c_int * m)(*[c for _, _, c in self.entries])
+        self.total = sum(c for _, _, c in self.entries)
+        h = C.c_void_p()
+        _check(self._lib.cub_graph_create(ctx._h, m, fams, dims, cnts,
+                                          C.byref(opts) if opts else None, C.byref(h)))
+        self._h = h
+        self._params = (GenzParams * self.total)()
+        self._er = (C.c_double * self.total)()
+        self._ea = (C.c_double * self.total)()
+        self._out = (CResult * self.total)()
+
+    def launch(self, integrands: Sequence[Integrand], epsrel, epsabs) -> list[Result]:
+        n = self.total
+        if len(integrands) != n:
+            raise ValueError(f"the graph integrates {n} integrals per launch")
+        k = 0
+        for fam, ndim, cnt in self.entries:
+            for f in integrands[k:k + cnt]:
+                if family_id(f.family) != family_id(fam) or f.ndim != ndim:
+                    raise ValueError("integrand does not match its graph entry")
+            k += cnt
+        for i, f in enumerate(integrands):
+            self._params[i] = f.params()
+            self._er[i] = float(epsrel if isinstance(epsrel, (int, float)) else epsrel[i])
+            self._ea[i] = float(epsabs if isinstance(epsabs, (int, float)) else epsabs[i])
+        rc = self._lib.cub_graph_launch(self._h, self._params, self._er, self._ea, self._out)
+        if rc < 0 and rc != ERR_CAPACITY:
+            raise CubatureError(rc, last_error())
+        return [Result.from_c(self._out[i]) for i in range(n)]
+
+    def info(self) -> tuple[int, int]:
+        """(replays, entries integrated again by the ordinary path)."""
+        a, b = C.c_longlong(), C.c_longlong()
+        _check(self._lib.cub_graph_info(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def close(self):
+        if self._h:
+            self._lib.cub_graph_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
 
 def spline_second_derivatives(xs, ys):
     """Natural cubic spline second derivatives (host), for device splines."""

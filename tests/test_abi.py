@@ -76,3 +76,16 @@ def test_no_device_reports_error(cub):
         pytest.skip("a device is present")
     with pytest.raises(cub.CubatureError):
         cub.Context(0)
+
+
+def test_graph_arguments_checked_before_the_device(cub):
+    """The graph entry points reject missing arguments without a device."""
+    lib = cub.load_library()
+    fams = (C.c_int * 1)(cub.family_id("gaussian"))
+    dims = (C.c_int * 1)(3)
+    cnts = (C.c_int * 1)(1)
+    h = C.c_void_p()
+    assert lib.cub_graph_create(None, 1, fams, dims, cnts, None, C.byref(h)) == cub.ERR_INVALID
+    assert lib.cub_graph_launch(None, None, None, None, None) == cub.ERR_INVALID
+    assert lib.cub_graph_info(None, None, None) == cub.ERR_INVALID
+    lib.cub_graph_destroy(None)

@@ -541,3 +541,81 @@ def test_mixed_batch_matches_single_family(cub, ctx):
         s = ctx.integrate_batch(f.family, 4, [f.params()], 1e-6, 1e-12)[0]
         assert m.status == s.status and m.nregions == s.nregions
         assert abs(m.integral - s.integral) <= 1e-13 * abs(s.integral) + 1e-15
+
+
+def _same(r, s, exact, label):
+    assert r.status == s.status and r.nregions == s.nregions and r.neval == s.neval, label
+    assert r.iterations == s.iterations, label
+    if exact:
+        assert r.integral == s.integral and r.error == s.error, label
+    else:
+        assert abs(r.integral - s.integral) <= 1e-13 * abs(s.integral) + 1e-300, label
+        assert abs(r.error - s.error) <= 1e-12 * abs(s.integral) + 1e-12 * s.error, label
+
+
+def test_graph_replays_match_direct_calls(cub, ctx):
+    """The default workload's two integrals captured once in a CUDA graph
+    and replayed with new parameters each call give the direct calls'
+    results (parameters read from device memory instead of kernel
+    arguments may change FMA contraction in the last bit)."""
+    g = ctx.graph([("oscillatory", 8, 1), ("corner_peak", 8, 1)])
+    try:
+        for a_osc, u_osc, a_cp in [(1.1, 0.3, 0.5), (0.9, 0.7, 0.8), (1.1, 0.3, 0.5)]:
+            fs = [cub.Integrand("oscillatory", 8, a_osc, u_osc),
+                  cub.Integrand("corner_peak", 8, a_cp, 0.0)]
+            got = g.launch(fs, 1e-6, 1e-12)
+            for f, r in zip(fs, got):
+                _same(r, ctx.integrate(f, 1e-6, 1e-12), False, f.family)
+        assert g.info() == (3, 0)
+    finally:
+        g.close()
+
+
+def test_graph_batch_entries_equal_batch_calls(cub, ctx):
+    """Batch entries (the same parameter source as cub_integrate_batch)
+    reproduce cub_integrate_batch bit for bit, per-integral tolerances
+    included, on two replays in a row."""
+    rng = np.random.default_rng(5)
+    g = ctx.graph([("product_peak", 4, 16), ("gaussian", 3, 2)])
+    try:
+        for rep in range(2):
+            pp = [cub.Integrand("product_peak", 4, list(np.exp(rng.uniform(0, np.log(30), 4))),
+                                list(rng.uniform(0.1, 0.9, 4))) for _ in range(16)]
+            ga = [cub.Integrand("gaussian", 3, list(rng.uniform(2, 8, 3)),
+                                list(rng.uniform(0.2, 0.8, 3))) for _ in range(2)]
+            er = list(rng.choice([1e-4, 1e-5], 18))
+            got = g.launch(pp + ga, er, 1e-12)
+            want = ctx.integrate_batch("product_peak", 4, [f.params() for f in pp], er[:16],
+                                       [1e-12] * 16)
+            want += ctx.integrate_batch("gaussian", 3, [f.params() for f in ga], er[16:],
+                                        [1e-12] * 2)
+            for k, (r, s) in enumerate(zip(got, want)):
+                _same(r, s, True, f"rep {rep} integral {k}")
+        assert g.info() == (2, 0)
+    finally:
+        g.close()
+
+
+def test_graph_finishes_through_batch_call(cub, ctx):
+    """An entry whose list outgrows the persistent limit inside the replay
+    is finished by cub_integrate_batch; the result is that call's."""
+    opts = cub.options(persistent_max_n=512)
+    f = cub.Integrand("product_peak", 6, 25.0, 0.4)
+    g = ctx.graph([("product_peak", 6, 1)], opts)
+    try:
+        r = g.launch([f], 1e-6, 1e-12)[0]
+        assert g.info() == (1, 1)
+        s = ctx.integrate_batch("product_peak", 6, [f.params()], 1e-6, 1e-12, opts)[0]
+        _same(r, s, True, "rerun")
+        assert r.nregions > 512
+    finally:
+        g.close()
+
+
+def test_graph_rejects_oversized_grid(cub, ctx):
+    """The initial grid must fit one persistent launch."""
+    with pytest.raises(cub.CubatureError) as e:
+        ctx.graph([("gaussian", 8, 4)], cub.options(persistent_max_n=512))
+    assert e.value.code == cub.ERR_UNSUPPORTED
+    with pytest.raises(cub.CubatureError):
+        ctx.graph([("gaussian", 1, 4)])
