@@ -1022,7 +1022,8 @@ __global__ void __launch_bounds__(256, 2) k_persistent(Src src, RuleTables T, Pe
     if (tracer) trace_mark(ctl, it, 2);
     cur ^= 1;
     prev_n = st.n;
-    if (blockIdx.x == 0 && threadIdx.x == 0) ctl->iters_done += 1;
+    // a store, not a read-modify-write: the launch starts at iter_base
+    if (blockIdx.x == 0 && threadIdx.x == 0) ctl->iters_done = p.iter_base + it + 1;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     ctl->cur = cur;

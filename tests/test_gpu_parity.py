@@ -612,6 +612,28 @@ def test_graph_finishes_through_batch_call(cub, ctx):
         g.close()
 
 
+def test_graph_finishes_phase2_through_batch_call(cub, ctx):
+    """Under the reference policy an entry whose integrals hand boxes to
+    phase 2 is finished by cub_integrate_batch (phase 2 is not part of the
+    graph); results equal that call's."""
+    opts = cub.options(phase1_cap=256)
+    fs = [cub.Integrand("product_peak", 4, a, 0.45) for a in (20.0, 30.0)]
+    g = ctx.graph([("product_peak", 4, 2)], opts)
+    try:
+        for rep in range(2):
+            got = g.launch(fs, 1e-7, 1e-12)
+            want = ctx.integrate_batch("product_peak", 4, [f.params() for f in fs], 1e-7, 1e-12,
+                                       opts)
+            for r, s in zip(got, want):
+                _same(r, s, True, f"rep {rep}")
+        assert g.info() == (2, 2)
+        ctx.reset_stats()
+        ctx.integrate_batch("product_peak", 4, [f.params() for f in fs], 1e-7, 1e-12, opts)
+        assert ctx.stats()["phase2_boxes"] > 0
+    finally:
+        g.close()
+
+
 def test_graph_rejects_oversized_grid(cub, ctx):
     """The initial grid must fit one persistent launch."""
     with pytest.raises(cub.CubatureError) as e:
