@@ -143,6 +143,9 @@ class Workspace {
 
   int device() const { return device_; }
   bool timing = false;  // record CUDA events around the rule, persistent and phase-2 kernels
+  // list capacity (2n + 32 per integral) that the widest iteration of the
+  // last run_batch needed
+  long long peak_need = 0;
   const std::string& error() const { return err_; }
   void set_error(const std::string& m) { err_ = m; }
   Stats& stats() { return stats_; }
@@ -642,6 +645,7 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
   long long n_cur = (long long)nint * padded;
   Stats& st = ws.stats();
 
+  ws.peak_need = 0;
   if (!ws.reserve_integrals(nint, s)) return kErrCuda;
   if (!ws.reserve_lists(N, std::min<long long>(std::max<long long>(1 << 20, 4 * n_cur), max_slots),
                         0, 0, s, max_slots))
@@ -685,6 +689,7 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
     n_cur = hs.n;
     // capacity for the worst case of the coming iteration(s)
     const long long need = 2 * n_cur + 32ll * nint;
+    ws.peak_need = std::max(ws.peak_need, need);
     if (need > max_slots) {
       status = kErrCapacity;
       break;

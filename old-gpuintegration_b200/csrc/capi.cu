@@ -320,7 +320,7 @@ int integrate_impl(cub_ctx* ctx, int family, int ndim, int count, const cub_genz
     }
     return dispatch_run(ctx, family, ndim, gn, hp.data(), d, ger.data(), gea.data(), o, gout,
                         lo ? gbox.data() : nullptr);
-  }, res);
+  }, res, ctx->ws);
   if (rc == kErrCuda) {
     set_error(ctx->ws->error());
     return CUB_ERR_CUDA;
@@ -613,7 +613,7 @@ int cub_integrate_mixed_batch(cub_ctx* ctx, int ndim, int count, const int* fami
       case 8: return run_mixed_dim_8(ctx, gn, ctx->d_params, ctx->d_fams, ger.data(), gea.data(), o, gout);
     }
     return (int)kErrInvalid;
-  }, res);
+  }, res, ctx->ws);
   if (rc != kOk && rc != kErrCapacity) return engine_status(ctx, rc);
   for (int k = 0; k < count; ++k) result_to_c(res[k], &out[k]);
   return engine_status(ctx, rc);

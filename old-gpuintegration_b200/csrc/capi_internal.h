@@ -66,27 +66,37 @@ CUB_DECLARE_DIM(8)
 // list.  run(idx, out) integrates the integrals idx (indices into the batch)
 // and returns an engine code.  Under the reference policy an integral's list
 // stays below 2 * phase1_cap + 96 slots, so groups of max_slots / that size
-// always fit.  Under the breadth policy lists are unbounded: the whole batch
-// is tried at once and integrals still running when the capacity ran out are
-// integrated again in groups a quarter the size (integrals are independent,
-// so a rerun gives the same result).  Returns kOk, kErrCapacity (some
-// integral never fit; its result is the last estimate) or the first error.
+// always fit.  Under the breadth policy lists are unbounded: with `ws` given
+// (the workspace run uses) and at least 4 * kProbeGroup integrals, the first
+// kProbeGroup integrals run as a group of their own, and later groups are
+// sized so that their widest iteration needs about 3/4 of max_slots at the
+// capacity per integral that the probe group needed; otherwise the whole
+// batch is tried at once.  Integrals still running when the capacity ran out
+// are integrated again in groups a quarter the size (integrals are
+// independent, so a rerun gives the same result).  Returns kOk,
+// kErrCapacity (some integral never fit; its result is the last estimate)
+// or the first error.
+constexpr int kProbeGroup = 256;
+
 template <class Run>
-int grouped_batch(int count, const Options& o, Run&& run, std::vector<Result>& res) {
+int grouped_batch(int count, const Options& o, Run&& run, std::vector<Result>& res,
+                  const Workspace* ws = nullptr) {
   res.assign(count, Result());
   int group = count;
-  if (o.policy == kPolicyReference && o.phase1_cap > 0) {
+  const bool bounded = o.policy == kPolicyReference && o.phase1_cap > 0;
+  if (bounded) {
     const long long per = 2ll * o.phase1_cap + 96;
     group = (int)std::max<long long>(1, std::min<long long>(count, o.max_slots / per));
   }
+  int probe = (!bounded && ws && o.max_slots > 0 && count >= 4 * kProbeGroup) ? kProbeGroup : 0;
   std::vector<int> todo(count), idx;
   for (int k = 0; k < count; ++k) todo[k] = k;
   std::vector<Result> gres;
   int rc = kOk;
   while (!todo.empty()) {
     std::vector<int> again;
-    for (size_t g0 = 0; g0 < todo.size(); g0 += group) {
-      const int gn = (int)std::min<size_t>(group, todo.size() - g0);
+    for (size_t g0 = 0; g0 < todo.size();) {
+      const int gn = (int)std::min<size_t>(probe ? probe : group, todo.size() - g0);
       idx.assign(todo.begin() + g0, todo.begin() + g0 + gn);
       gres.assign(gn, Result());
       const int r = run(idx, gres.data());
@@ -97,6 +107,14 @@ int grouped_batch(int count, const Options& o, Run&& run, std::vector<Result>& r
           again.push_back(idx[j]);
       }
       if (r == kErrCapacity && (group == 1 || again.empty())) rc = kErrCapacity;
+      if (probe) {
+        probe = 0;
+        if (r == kOk && ws->peak_need > 0) {
+          const long long per = std::max<long long>(1, ws->peak_need / gn);
+          group = (int)std::max<long long>(1, std::min<long long>(count, o.max_slots * 3 / 4 / per));
+        }
+      }
+      g0 += gn;
     }
     todo.swap(again);
     group = std::max(1, group / 4);

@@ -143,7 +143,7 @@ int cub_integrate_table7_batch(cub_ctx* ctx, const cub_table7* tables, int count
                         ctx->stream) != cudaSuccess)
       return (int)kErrCuda;
     return run_batch<7>(*ctx->ws, src, gn, ger.data(), gea.data(), o, gout, ctx->stream);
-  }, res);
+  }, res, ctx->ws);
   if (rc != kOk && rc != kErrCapacity) return engine_status(ctx, rc);
   for (int k = 0; k < count; ++k) result_to_c(res[k], &out[k]);
   return engine_status(ctx, rc);
