@@ -35,11 +35,37 @@ __host__ __device__ __forceinline__ int table_cell(const double* xs, int n, doub
   return lo - 1;
 }
 
+// Lookup hint of a knot array: x0 and 1 / spacing for knots that are
+// uniform to rounding (inv_dx = 0: no hint).  Set on the host.
+struct KnotHint {
+  double x0 = 0;
+  double inv_dx = 0;
+};
+
+// table_cell from a guess: cell floor((t - x0) / dx), corrected by walking
+// down while xs[g - 1] >= t and up while xs[g] < t.  The predicate
+// xs[i] >= t is monotone in i for ascending knots, so the walk ends on the
+// binary search's answer whatever the guess; a hint only saves reads (two
+// independent ones on a uniform table instead of log2(n) dependent ones).
+// NaN takes the binary search.
+__host__ __device__ __forceinline__ int table_cell(const double* xs, int n, double t,
+                                                   const KnotHint& h) {
+  const double u = (t - h.x0) * h.inv_dx;
+  if (h.inv_dx > 0 && u == u) {
+    int g = u < 0 ? 1 : (u >= (double)(n - 2) ? n - 1 : (int)u + 1);
+    while (g > 1 && xs[g - 1] >= t) --g;
+    while (g < n - 1 && xs[g] < t) ++g;
+    return g - 1;
+  }
+  return table_cell(xs, n, t);
+}
+
 struct Interp2D {
   const double* xs;  // row coordinates, nx, ascending
   const double* ys;  // column coordinates, ny, ascending
   const double* zs;  // values, row-major: zs[i * ny + j] at (xs[i], ys[j])
   int nx, ny;
+  KnotHint hx, hy;
 
   // Value at (x, y) in a known cell (i, j).
   __host__ __device__ __forceinline__ double at_cell(int i, int j, double x, double y) const {
@@ -52,7 +78,7 @@ struct Interp2D {
   }
 
   __host__ __device__ __forceinline__ double operator()(double x, double y) const {
-    return at_cell(table_cell(xs, nx, x), table_cell(ys, ny, y), x, y);
+    return at_cell(table_cell(xs, nx, x, hx), table_cell(ys, ny, y, hy), x, y);
   }
 };
 
@@ -61,9 +87,10 @@ struct Spline1D {
   const double* ys;  // values
   const double* y2;  // second derivatives (natural spline: y2[0] = y2[n-1] = 0)
   int n;
+  KnotHint h;
 
   __host__ __device__ __forceinline__ double operator()(double t) const {
-    const int i = table_cell(xs, n, t);
+    const int i = table_cell(xs, n, t, h);
     const double h = xs[i + 1] - xs[i];
     const double a = (xs[i + 1] - t) / h, b = (t - xs[i]) / h;
     return a * ys[i] + b * ys[i + 1] +
@@ -81,10 +108,11 @@ struct LcLt {
   const double* ys;  // zt knots
   const double* z[5];  // tau, mu, sigma, fmsk, fprj, each row-major nx x ny
   int nx, ny;
+  KnotHint hx, hy;
 
   __device__ __forceinline__ double operator()(const double* x) const {
     const double lt = x[0], zt = x[1], lc = x[2];
-    const int i = table_cell(xs, nx, lt), j = table_cell(ys, ny, zt);
+    const int i = table_cell(xs, nx, lt, hx), j = table_cell(ys, ny, zt, hy);
     double v[5];
 #pragma unroll
     for (int q = 0; q < 5; ++q) v[q] = Interp2D{xs, ys, z[q], nx, ny}.at_cell(i, j, lt, zt);
