@@ -35,7 +35,7 @@ __device__ __forceinline__ float silu_grad(float z) {
   return s * (1.0f + z * (1.0f - s));
 }
 
-enum Epilogue : int { kEpiStore = 0, kEpiForward = 1, kEpiBackward = 2, kEpiInfer = 3 };
+enum Epilogue : int { kEpiStore = 0, kEpiForward = 1, kEpiBackward = 2 };
 
 struct EpiArgs {
   // kEpiStore: out[e * batch_out + row * ld_out + col] (fp32)
@@ -71,14 +71,6 @@ __device__ __forceinline__ void epilogue(const EpiArgs& ep, int e, int row, int 
       ep.z[ra + i] = zb;
       ep.h[ra + i] = hb;
       ep.ht[rt + (long long)(c0 + i) * ep.ld_t] = hb;
-    }
-  } else if (EPI == kEpiInfer) {
-    // forward without the training copies: H only (same roundings)
-    const float* b = ep.bias + (long long)e * ep.batch_bias + c0;
-    const long long ra = (long long)e * ep.batch_act + (long long)row * ep.ld_act + c0;
-    for (int i = 0; i < cnt; ++i) {
-      const __nv_bfloat16 zb = __float2bfloat16(v[i] + b[i]);
-      ep.h[ra + i] = __float2bfloat16(silu(__bfloat162float(zb)));
     }
   } else {
     const long long ra = (long long)e * ep.batch_act + (long long)row * ep.ld_act + c0;

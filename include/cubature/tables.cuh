@@ -115,7 +115,7 @@ struct LcLt {
     const int i = table_cell(xs, nx, lt, hx), j = table_cell(ys, ny, zt, hy);
     double v[5];
 #pragma unroll
-    for (int q = 0; q < 5; ++q) v[q] = Interp2D{xs, ys, z[q], nx, ny}.at_cell(i, j, lt, zt);
+    for (int q = 0; q < 5; ++q) v[q] = Interp2D{xs, ys, z[q], nx, ny, hx, hy}.at_cell(i, j, lt, zt);
     const double tau = v[0], mu = v[1], sigma = v[2], fmsk = v[3], fprj = v[4];
     const double exptau = exp(tau * (2.0 * mu + tau * sigma * sigma - 2.0 * lc) / 2.0);
     const double r2s = sqrt(2.0) * sigma;

@@ -143,12 +143,10 @@ int cub_integrate_table7_batch(cub_ctx* ctx, const cub_table7* tables, int count
   }
   detail::Table7Source src;
   src.base.spline = Spline1D{tables->spline.xs, tables->spline.ys, tables->spline.y2,
-                             tables->spline.n};
+                             tables->spline.n, knot_hint(tables->spline.xs, tables->spline.n)};
   src.base.grid = Interp2D{tables->grid.xs, tables->grid.ys, tables->grid.zs, tables->grid.nx,
-                           tables->grid.ny};
-  src.base.spline.h = knot_hint(tables->spline.xs, tables->spline.n);
-  src.base.grid.hx = knot_hint(tables->grid.xs, tables->grid.nx);
-  src.base.grid.hy = knot_hint(tables->grid.ys, tables->grid.ny);
+                           tables->grid.ny, knot_hint(tables->grid.xs, tables->grid.nx),
+                           knot_hint(tables->grid.ys, tables->grid.ny)};
   src.base.inv2s2 = 1.0 / (2.0 * tables->sigma * tables->sigma);
   src.base.offset = 0;
   src.offsets = ctx->d_aux;

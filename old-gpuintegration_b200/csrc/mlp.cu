@@ -434,35 +434,6 @@ namespace {
 constexpr int kCvDim = 7;
 using CvPT = detail::PointTable<kCvDim>;
 
-// Network inputs at every rule point of slots [s0, s0 + n) of the current
-// list (row (s - s0) * npts + p), the same arithmetic as the rule:
-// x_i = fma(c, len, lo); padding slots and rows past n * npts (up to `rows`)
-// are zero.
-__global__ void k_cv_nodes(const double* lo, const double* len, const int* rid, long long cap,
-                           long long s0, long long n, long long rows, bf16* X) {
-  __shared__ CvPT pt;
-  pt.fill(threadIdx.x, blockDim.x);
-  __syncthreads();
-  const long long used = n * CvPT::kPoints;
-  for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < rows;
-       r += (long long)gridDim.x * blockDim.x) {
-    const long long s = s0 + r / CvPT::kPoints;
-    const int p = (int)(r % CvPT::kPoints);
-    const bool live = r < used && rid[s] >= 0;
-    const uint2 e = live ? pt.ent[p] : make_uint2(0, 0);
-#pragma unroll
-    for (int i = 0; i < mlp::kInPad; ++i) {
-      float v = 0.0f;
-      if (live && i < kCvDim) {
-        const double x = fma(pt.ctab[(e.x >> (4 * i)) & 15u], len[(long long)i * cap + s],
-                             lo[(long long)i * cap + s]);
-        v = (float)(2.0 * x - 1.0);
-      }
-      X[r * mlp::kInPad + i] = __float2bfloat16(v);
-    }
-  }
-}
-
 // f at points x [E][S][7] for integral e's parameters -> y [E][S].
 template <class F>
 __global__ void k_eval_points(const GenzParams* params, const double* x, long long S, double* y) {
@@ -620,41 +591,6 @@ __global__ void __launch_bounds__(256) k_cv_smooth(const float* P, const bf16* W
     if (lane == 0) g[r] = (double)scale * (double)(acc + b3);
     __syncwarp();
   }
-}
-
-// g of network `net_k` at `rows` rows of X (multiple of 128): three GEMM
-// layers on the tensor cores through two ping-pong buffers, then the output
-// layer; g_out[r] for r < valid.
-int forward_one(cub_mlp* m, int net_k, const bf16* X, long long rows, long long valid, bf16* Ha,
-                bf16* Hb, double* g_out, cudaStream_t s) {
-  const dim3 grid((unsigned)(rows / umma::kTileM), 1, 1);
-  umma::GemmArgs g{};
-  g.error = m->err;
-  g.m = (int)rows;
-  mlp::EpiArgs ep{};
-  ep.ld_act = 128;
-  ep.batch_act = 0;
-  const long long P = Layout::kCount;
-  const bf16* in[3] = {X, Ha, Hb};
-  bf16* out[3] = {Ha, Hb, Ha};
-  const bf16* w[3] = {m->W0 + (long long)net_k * 128 * 16, m->W1 + (long long)net_k * 128 * 128,
-                      m->W2 + (long long)net_k * 128 * 128};
-  const int boff[3] = {Layout::B0, Layout::B1, Layout::B2};
-  for (int l = 0; l < 3; ++l) {
-    g.a = in[l];
-    g.lda = l == 0 ? mlp::kInPad : 128;
-    g.b = w[l];
-    g.ldb = l == 0 ? mlp::kInPad : 128;
-    g.k = l == 0 ? mlp::kInPad : 128;
-    ep.bias = m->P + net_k * P + boff[l];
-    ep.h = out[l];
-    cudaError_t e = launch_gemm<128, mlp::kEpiInfer>(grid, s, g, ep);
-    if (e != cudaSuccess) return cuda_error(e, "inference GEMM");
-  }
-  mlp::k_output<<<dim3((unsigned)(rows / 128), 1, 1), 128, 0, s>>>(
-      m->P + net_k * P, Ha, nullptr, nullptr, 0, 0.0f, nullptr, nullptr, nullptr, rows, valid,
-      m->scale + net_k, g_out, 0);
-  return check(cudaGetLastError(), "k_output");
 }
 
 // Evaluation hook of the engine's multi-launch driver: the rule over the
