@@ -72,8 +72,10 @@ CUB_DECLARE_DIM(8)
 // sized so that their widest iteration needs about 3/4 of max_slots at the
 // capacity per integral that the probe group needed; otherwise the whole
 // batch is tried at once.  Integrals still running when the capacity ran out
-// are integrated again in groups a quarter the size (integrals are
-// independent, so a rerun gives the same result).  Returns kOk,
+// are integrated again in groups a quarter the size.  Integrals are
+// independent, so a rerun gives the same result up to the order in which
+// points are summed: the list length of a group decides whether the
+// persistent or the multi-launch rule kernel evaluates an iteration.  Returns kOk,
 // kErrCapacity (some integral never fit; its result is the last estimate)
 // or the first error.
 constexpr int kProbeGroup = 256;

@@ -236,6 +236,31 @@ def test_batch_matches_single(cub, oracle, ctx):
         assert b.nregions == s.nregions and b.status == s.status
 
 
+def test_grouped_breadth_batch_equals_one_group(cub, ctx):
+    """A breadth-policy batch of 1100 integrals under a small region capacity
+    runs as a 256-integral probe group and groups sized from its peak (plus
+    reruns in smaller groups if one still overflows).  Integrals share no
+    arithmetic, but the group size decides which kernel evaluates an
+    iteration (the persistent kernel for short lists, the multi-launch rule
+    kernel for long ones), and the two sum a region's points in different
+    orders: results agree with the default-capacity run to that rounding."""
+    rng = np.random.default_rng(11)
+    n, count, eps = 4, 1100, 1e-4
+    params = [cub.make_params(n, list(np.exp(rng.uniform(0, np.log(20), n))),
+                              list(rng.uniform(0.1, 0.9, n))) for _ in range(count)]
+    whole = ctx.integrate_batch("product_peak", n, params, eps, 1e-12,
+                                cub.options(policy=cub.POLICY_BREADTH))
+    ctx.reset_stats()
+    grouped = ctx.integrate_batch("product_peak", n, params, eps, 1e-12,
+                                  cub.options(policy=cub.POLICY_BREADTH, max_slots=1 << 19))
+    assert ctx.stats()["persistent_launches"] + ctx.stats()["eval_launches"] > 0
+    for k, (g, w) in enumerate(zip(grouped, whole)):
+        assert g.status == w.status, k
+        assert abs(g.integral - w.integral) <= 1e-3 * eps * abs(w.integral) + 1e-15, k
+        assert abs(g.nregions - w.nregions) <= 0.01 * w.nregions + 4, k
+    assert all(r.status == 0 for r in whole)
+
+
 def test_batch_matches_oracle(cub, oracle, ctx):
     rng = np.random.default_rng(5)
     n, eps = 6, 1e-4
