@@ -109,6 +109,7 @@ class Workspace {
     bytes_ = 0;
     if (host_block_) cudaFreeHost(host_block_);
     host_block_ = nullptr;
+    host_block_dev_ = nullptr;
     ctl_host_ = nullptr;
     ist_host_ = nullptr;
     ctl_block_ = nullptr;
@@ -181,6 +182,16 @@ class Workspace {
   IntegralState* ist_host_ = nullptr;
   static constexpr size_t kStateOffset = (sizeof(Control) + 255) & ~size_t(255);
   size_t state_bytes(int nint) const { return kStateOffset + sizeof(IntegralState) * nint; }
+  // Device address of the pinned state copy, when a persistent launch of
+  // nint integrals should write its final states there itself (small
+  // batches: one block stores them in less time than a copy takes to
+  // start); null otherwise.
+  static constexpr int kDirectStatesMax = 64;
+  static_assert(sizeof(IntegralState) % 8 == 0 && kStateOffset % 8 == 0,
+                "the kernel stores the states as 8-byte words");
+  Control* direct_states(int nint) const {
+    return nint <= kDirectStatesMax ? static_cast<Control*>(host_block_dev_) : nullptr;
+  }
   void* slab = nullptr;
   int* heap = nullptr;
   int* counter = nullptr;
@@ -350,12 +361,19 @@ class Workspace {
     free_buf(int_cnt);
     if (host_block_) cudaFreeHost(host_block_);
     host_block_ = nullptr;
+    host_block_dev_ = nullptr;
     ctl_host_ = nullptr;
     ist_host_ = nullptr;
     nint_cap_ = 0;
     const int n = std::max(nint, 64);
     if (!alloc(&ctl_block_, state_bytes(n)) || !alloc(&int_cnt, sizeof(unsigned) * n)) return false;
-    if (!ck(cudaMallocHost(&host_block_, state_bytes(n)))) return false;
+    // mapped, so that a persistent launch can write its final states here
+    // itself; without a device address the copy engine does it
+    if (!ck(cudaHostAlloc(&host_block_, state_bytes(n), cudaHostAllocMapped))) return false;
+    if (cudaHostGetDevicePointer(&host_block_dev_, host_block_, 0) != cudaSuccess) {
+      host_block_dev_ = nullptr;
+      cudaGetLastError();
+    }
     ctl = static_cast<Control*>(ctl_block_);
     ist = reinterpret_cast<IntegralState*>(static_cast<char*>(ctl_block_) + kStateOffset);
     ctl_host_ = static_cast<Control*>(host_block_);
@@ -428,6 +446,7 @@ class Workspace {
   size_t box_cap_ = 0;
   void* ctl_block_ = nullptr;
   void* host_block_ = nullptr;
+  void* host_block_dev_ = nullptr;  // device address of host_block_ (mapped)
   size_t bytes_ = 0;
   std::string err_;
   Stats stats_;
@@ -599,6 +618,8 @@ inline PersistArgs persist_args(const Workspace& ws, const EngineArgs& a, const 
   p.per_integral = per;
   p.padded = padded;
   p.box = d_box;
+  p.host_out = nullptr;
+  p.host_words = 0;
   return p;
 }
 
@@ -712,6 +733,8 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
       st.h2d_bytes += (long long)up;
       PersistArgs p = detail::persist_args(ws, a, opt, c0.iters_done, pmax, grid_pending, dv,
                                            per, padded, d_box);
+      p.host_out = ws.direct_states(nint);
+      p.host_words = (int)(ws.state_bytes(nint) / 8);
       grid_pending = false;
       void* args[] = {(void*)&src, (void*)&T, (void*)&p};
       if (ws.timing) ws.ck(cudaEventRecord(ws.ev[0], s));
@@ -721,10 +744,11 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
       if (ws.timing) ws.ck(cudaEventRecord(ws.ev[1], s));
       st.launches += 1;
       st.persistent_launches += 1;
-      // the states come back with the control block: when the launch
-      // finished every integral, no further round trip is needed
-      if (!ws.ck(cudaMemcpyAsync(ws.ctl_host_, ws.ctl, ws.state_bytes(nint),
-                                 cudaMemcpyDeviceToHost, s)))
+      // the states come back with the control block (stored by the kernel
+      // itself for small batches): when the launch finished every
+      // integral, no further round trip is needed
+      if (!p.host_out && !ws.ck(cudaMemcpyAsync(ws.ctl_host_, ws.ctl, ws.state_bytes(nint),
+                                                cudaMemcpyDeviceToHost, s)))
         return kErrCuda;
       if (!ws.ck(cudaStreamSynchronize(s))) return kErrCuda;
       st.d2h_bytes += (long long)ws.state_bytes(nint);
@@ -922,6 +946,8 @@ int replay_prepare(Workspace& ws, int nint, const Options& opt, cudaStream_t s, 
   r->padded = padded;
   r->n0 = n0;
   r->p = detail::persist_args(ws, a, opt, 0, pmax, true, dv, per, padded, nullptr);
+  r->p.host_out = ws.direct_states(nint);
+  r->p.host_words = (int)(ws.state_bytes(nint) / 8);
   return kOk;
 }
 
@@ -953,7 +979,8 @@ int replay_enqueue(Workspace& ws, const Src& src, const Replay& r, cudaStream_t 
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   if (!ws.ck(cudaLaunchKernelEx(&cfg, k_persistent<N, Src>, src, T, r.p))) return kErrCuda;
-  if (!ws.ck(cudaMemcpyAsync(ws.ctl_host_, ws.ctl, bytes, cudaMemcpyDeviceToHost, s)))
+  if (!r.p.host_out &&
+      !ws.ck(cudaMemcpyAsync(ws.ctl_host_, ws.ctl, bytes, cudaMemcpyDeviceToHost, s)))
     return kErrCuda;
   return kOk;
 }

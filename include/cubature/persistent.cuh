@@ -60,6 +60,11 @@ struct PersistArgs {
   int init;
   int divisions, per_integral, padded;
   const double* box;
+  // When set (mapped pinned memory): at exit block 0 also stores the
+  // control block and the integral states, host_words 8-byte words, there,
+  // and the host needs no copy back.
+  Control* host_out;
+  int host_words;
 };
 
 // How the first step of an iteration obtains a slot's region.
@@ -1025,13 +1030,23 @@ __global__ void __launch_bounds__(256, 2) k_persistent(Src src, RuleTables T, Pe
     // a store, not a read-modify-write: the launch starts at iter_base
     if (blockIdx.x == 0 && threadIdx.x == 0) ctl->iters_done = p.iter_base + it + 1;
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    ctl->cur = cur;
-    IterState h = st;
-    h.overflow = 0;
-    h.handoff = 0;
-    ctl->host = h;
-    ctl->exit_reason = reason;
+  if (blockIdx.x == 0) {
+    if (threadIdx.x == 0) {
+      ctl->cur = cur;
+      IterState h = st;
+      h.overflow = 0;
+      h.handoff = 0;
+      ctl->host = h;
+      ctl->exit_reason = reason;
+    }
+    if (p.host_out) {
+      // the states were completed before the last grid barrier; the
+      // control block's final fields just above
+      __syncthreads();
+      const unsigned long long* src = reinterpret_cast<const unsigned long long*>(ctl);
+      unsigned long long* dst = reinterpret_cast<unsigned long long*>(p.host_out);
+      for (int i = threadIdx.x; i < p.host_words; i += blockDim.x) dst[i] = src[i];
+    }
   }
 }
 
