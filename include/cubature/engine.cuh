@@ -846,7 +846,8 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
     blocks = std::max<long long>(blocks, 1);
     const long long nwarps = blocks * 4;
     const int stride = opt.phase2_max_regions + 2;
-    if (!ws.reserve_slab(sizeof(P2Region<N>) * nwarps * stride, (size_t)nwarps * stride))
+    if (!ws.reserve_slab(sizeof(P2Region<N>) * nwarps * stride,
+                         (size_t)nwarps * stride * (sizeof(P2HeapEnt) / sizeof(int))))
       return kErrCuda;
     if (!ws.ck(cudaMemsetAsync(ws.counter, 0, sizeof(int), s))) return kErrCuda;
     Phase2Args p;
@@ -857,7 +858,7 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
     p.n_left = (int)n_left;
     p.max_regions = opt.phase2_max_regions;
     p.slab = ws.slab;
-    p.heap = ws.heap;
+    p.heap = reinterpret_cast<P2HeapEnt*>(ws.heap);
     p.next_box = ws.counter;
     p.out = ws.left_res;
     p.ist = ws.ist;

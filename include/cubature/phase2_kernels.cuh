@@ -7,7 +7,8 @@
 //
 // Re-design for sm_100a: one warp per leftover box, persistent warps pulling
 // boxes from an atomic counter.  Each step bisects the box's exact maximum
-// error subregion (a binary heap kept by lane 0), and the two children are
+// error subregion (a binary heap kept by lane 0, each entry holding the
+// subregion's error beside its index), and the two children are
 // evaluated in parallel by the two 16-lane halves of the warp.  Subregions
 // live in a per-warp slab of global memory preallocated by the host, so
 // there is no device malloc and the footprint is fixed by the grid size.
@@ -31,6 +32,15 @@ struct P2Region {
   double lo[N], hi[N];
 };
 
+// Heap entry: a subregion's error (the key) beside its pool index, so that
+// a heap level costs one read, not a read of the index and a dependent read
+// of the subregion.
+struct P2HeapEnt {
+  double err;
+  int idx;
+  int pad;
+};
+
 struct Phase2Args {
   const double* left_lo;  // [N][left_cap]
   const double* left_len;
@@ -39,7 +49,7 @@ struct Phase2Args {
   int n_left;
   int max_regions;  // bisections per box (MAX_GLOBALPOOL_SIZE, quad.h:9)
   void* slab;       // per-warp pools: nwarps * (max_regions + 2) regions
-  int* heap;        // per-warp heaps: nwarps * (max_regions + 2) ints
+  P2HeapEnt* heap;  // per-warp heaps: nwarps * (max_regions + 2) entries
   int* next_box;    // work counter
   LeftoverResult* out;
   const IntegralState* ist;
@@ -47,36 +57,42 @@ struct Phase2Args {
 
 namespace detail {
 
-template <int N>
-__device__ __forceinline__ void heap_push(P2Region<N>* pool, int* heap, int& hn, int idx) {
+// Max-heap on the error, sifting with a hole: the same comparisons, and so
+// the same order, as swapping the entries level by level.
+__device__ __forceinline__ void heap_push(P2HeapEnt* heap, int& hn, int idx, double err) {
   int i = hn++;
-  heap[i] = idx;
+  const P2HeapEnt e{err, idx, 0};
   while (i > 0) {
     const int p = (i - 1) / 2;
-    if (pool[heap[p]].err >= pool[heap[i]].err) break;
-    const int t = heap[p];
-    heap[p] = heap[i];
-    heap[i] = t;
+    const P2HeapEnt pe = heap[p];
+    if (pe.err >= e.err) break;
+    heap[i] = pe;
     i = p;
   }
+  heap[i] = e;
 }
 
-template <int N>
-__device__ __forceinline__ int heap_pop(P2Region<N>* pool, int* heap, int& hn) {
-  const int top = heap[0];
-  heap[0] = heap[--hn];
+__device__ __forceinline__ int heap_pop(P2HeapEnt* heap, int& hn) {
+  const int top = heap[0].idx;
+  const P2HeapEnt e = heap[--hn];
   int i = 0;
   for (;;) {
     const int l = 2 * i + 1, r = l + 1;
     int m = i;
-    if (l < hn && pool[heap[l]].err > pool[heap[m]].err) m = l;
-    if (r < hn && pool[heap[r]].err > pool[heap[m]].err) m = r;
+    double km = e.err;
+    if (l < hn) {
+      const double kl = heap[l].err;
+      if (kl > km) {
+        m = l;
+        km = kl;
+      }
+    }
+    if (r < hn && heap[r].err > km) m = r;
     if (m == i) break;
-    const int t = heap[m];
-    heap[m] = heap[i];
-    heap[i] = t;
+    heap[i] = heap[m];
     i = m;
   }
+  heap[i] = e;
   return top;
 }
 
@@ -122,7 +138,7 @@ __global__ void __launch_bounds__(128) k_phase2(Src src, RuleTables T, Phase2Arg
   const long long gwarp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / 32;
   const int stride = a.max_regions + 2;
   P2Region<N>* pool = reinterpret_cast<P2Region<N>*>(a.slab) + gwarp * stride;
-  int* heap = a.heap + gwarp * stride;
+  P2HeapEnt* heap = a.heap + gwarp * stride;
 
   for (;;) {
     int box = 0;
@@ -156,7 +172,7 @@ __global__ void __launch_bounds__(128) k_phase2(Src src, RuleTables T, Phase2Arg
     double ERR = r0.err, RESULT = r0.avg;
     if (lane == 0) {
       pool[0] = r0;
-      detail::heap_push<N>(pool, heap, hn, 0);
+      detail::heap_push(heap, hn, 0, r0.err);
     }
     __syncwarp();
     int nreg = 1;
@@ -164,7 +180,7 @@ __global__ void __launch_bounds__(128) k_phase2(Src src, RuleTables T, Phase2Arg
            (nreg == 1 || ERR > detail::max_err(RESULT, epsrel, epsabs));
          ++nreg) {
       int pi = 0;
-      if (lane == 0) pi = detail::heap_pop<N>(pool, heap, hn);
+      if (lane == 0) pi = detail::heap_pop(heap, hn);
       pi = __shfl_sync(0xffffffffu, pi, 0);
       __syncwarp();
       const P2Region<N> parent = pool[pi];
@@ -214,8 +230,8 @@ __global__ void __launch_bounds__(128) k_phase2(Src src, RuleTables T, Phase2Arg
         right.axis = axR;
         pool[pi] = left;
         pool[used] = right;
-        detail::heap_push<N>(pool, heap, hn, pi);
-        detail::heap_push<N>(pool, heap, hn, used);
+        detail::heap_push(heap, hn, pi, errL);
+        detail::heap_push(heap, hn, used, errR);
       }
       ++used;
       ERR = __shfl_sync(0xffffffffu, ERR, 0);
