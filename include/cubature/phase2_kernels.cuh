@@ -126,8 +126,11 @@ __device__ __forceinline__ RegionResult eval_sub(const F& f, const double (&BL)[
 
 }  // namespace detail
 
+// Three blocks (12 warps) per SM: each warp refines its box serially, so
+// warps in flight hide the latency of the heap and the rule; the register
+// cap this sets costs a few spilled words.
 template <int N, class Src>
-__global__ void __launch_bounds__(128) k_phase2(Src src, RuleTables T, Phase2Args a) {
+__global__ void __launch_bounds__(128, 3) k_phase2(Src src, RuleTables T, Phase2Args a) {
   __shared__ detail::ItemTable<N> tab;
   if (threadIdx.x == 0) tab.fill();
   __syncthreads();
