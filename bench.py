@@ -62,9 +62,12 @@ WORKLOADS = {
     },
     # 256 x the 7-D table integrand: 512-knot spline x 128 x 128 bilinear x
     # Gaussian kernel (sigma 0.25), mu offsets uniform in [-1, 1]; FP64
-    # tables (seeded synthetic data, cubature.tables); breadth-first
+    # tables (seeded synthetic data, cubature.tables); breadth-first.
+    # epsabs 1e-15: the per-region absolute allowance summed over the ~2e7
+    # regions stays far below epsrel |I| (1e-12 lets the result drift ~3e-6
+    # from the closed-form value, inside its error estimate)
     "table7_7d_batch": {
-        "tables": ("table7", 7, 256), "epsrel": 1e-6, "epsabs": 1e-12, "policy": "breadth",
+        "tables": ("table7", 7, 256), "epsrel": 1e-6, "epsabs": 1e-15, "policy": "breadth",
     },
     # learned control variate on 7-D product peaks (the batch generator at
     # n = 7): network trained on the tensor cores, integral of f - g plus
@@ -286,6 +289,61 @@ def cpu_table7_rate(workload: dict, seconds: float, threads: int = 0,
     return rate, evals / el, cores, done, el
 
 
+def cpu_model() -> str:
+    """The host CPU's model name (/proc/cpuinfo), or the platform string."""
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+
+    return platform.processor() or platform.machine()
+
+
+REF_DRIVER = ROOT / "oracle" / "_ref" / "ref_driver"
+FAMILY_IDS = {"gaussian": 1, "oscillatory": 2, "corner_peak": 3, "product_peak": 4,
+              "continuous": 5, "discontinuous": 6, "cossum": 7}
+
+
+def reference_gpu_rate(workload: dict, warmup: int, reps: int, device: int):
+    """The unmodified reference engine (quad::GPUcuhre compiled from its own
+    sources by oracle/ref_driver/Makefile) on the same integrands, one
+    process on this GPU: warm median ms per integrate() call, summed over
+    the step's integrands.  None when the driver was not built or fails."""
+    if "items" not in workload or not REF_DRIVER.exists():
+        return None
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES=os.environ.get("CUDA_VISIBLE_DEVICES",
+                                                                 str(device)).split(",")[0])
+    per, total_ms = [], 0.0
+    for fam, n, a, u in workload["items"]:
+        av = a if isinstance(a, (list, tuple)) else [a] * n
+        uv = u if isinstance(u, (list, tuple)) else [u] * n
+        cmd = [str(REF_DRIVER), "bench", str(FAMILY_IDS[fam]), str(n), repr(workload["epsrel"]),
+               repr(workload["epsabs"]), str(warmup), str(reps)] + [repr(float(x)) for x in av]
+        cmd += [repr(float(x)) for x in uv]
+        try:
+            out = subprocess.run(cmd, capture_output=True, text=True, timeout=300, env=env)
+        except (OSError, subprocess.TimeoutExpired):
+            return None
+        rec = None
+        for line in out.stdout.splitlines():
+            if line.startswith("BENCH "):
+                rec = json.loads(line[6:])
+        if out.returncode != 0 or rec is None:
+            return None
+        per.append({"family": fam, "ndim": n, "median_ms": rec["median_ms"],
+                    "min_ms": rec["min_ms"], "nregions": rec["nregions"],
+                    "errorFlag": rec["errorFlag"], "integral": rec["integral"]})
+        total_ms += rec["median_ms"]
+    return {"value": len(per) / (total_ms / 1e3), "unit": "integrals/s",
+            "ms_per_step": total_ms, "per_integrand": per, "reps": reps, "warmup": warmup,
+            "source": "unmodified reference engine (quad::GPUcuhre) built from its sources by "
+                      "oracle/ref_driver/Makefile; warm median of steady-clock times around "
+                      "integrate(), device synchronised on both sides"}
+
+
 def cpu_sample_text(workload: dict, done: int, el: float,
                     regions_per_integral: float | None = None) -> str:
     if "tables" in workload:
@@ -336,6 +394,8 @@ def main() -> int:
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="oscillatory_cornerpeak_8d")
     ap.add_argument("--cpu-seconds", type=float, default=8.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-ref-gpu", action="store_true",
+                    help="skip timing the reference engine on the GPU beside the run")
     ap.add_argument("--count", type=int, default=0,
                     help="batch workloads: integrals per step (default: the workload's)")
     args = ap.parse_args()
@@ -427,7 +487,11 @@ def main() -> int:
                                               opts)
 
         fams = [(fam, n)] * len(offs)
-        exact = [None] * len(offs)  # no closed form: convergence status is checked
+        import oracle as O
+
+        d7 = T.table7_data(0)
+        exact = [O.table7_exact(d7["spline_x"], d7["spline_y"], d7["grid_x"], d7["grid_y"],
+                                d7["grid_z"], d7["sigma"], o) for o in offs]
     else:
         # weak scaling: `count` integrals per rank; the job's world * count
         # integrals (seed = global index) are cut into contiguous shards
@@ -448,6 +512,27 @@ def main() -> int:
 
     for _ in range(args.warmup):
         step()
+    torch.cuda.synchronize()
+
+    # regions per (family, ndim) in the persistent kernels and in the
+    # multi-launch rule kernel, from one untimed step with the counters read
+    # after each call
+    split = {}
+
+    def add_split(key, total, s0):
+        pk, ml = s0["persistent_regions"], s0["regions_evaluated"]
+        a, b, c = split.get(key, (0, 0, 0))
+        split[key] = (a + pk, b + ml, c + max(0, total - pk - ml))
+
+    if "items" in workload:
+        for f, key in zip(items, fams):
+            ctx.reset_stats()
+            r = ctx.integrate(f, workload["epsrel"], workload["epsabs"], opts)
+            add_split(key, r.nregions, ctx.stats())
+    else:
+        ctx.reset_stats()
+        res0 = step()
+        add_split(fams[0], sum(r.nregions for r in res0), ctx.stats())
     torch.cuda.synchronize()
 
     ctx.reset_stats()
@@ -528,13 +613,18 @@ def main() -> int:
                      "regions": int(sum(r.nregions for r in plain_res)),
                      "cv_stats": dict(cv_stats)}
 
-    # correctness of the last step against the analytic integrals
+    # correctness of the last step against the analytic (or closed-form)
+    # integrals: an integral counts when it converged (status 0) and lies
+    # within epsrel of the true value; the looser 2 epsrel count is reported
+    # beside it
     nint = len(results)
-    bad = 0
+    bad = bad2 = 0
     for r, ex in zip(results, exact):
-        if not (r.status == 0 and (ex is None or
-                                   abs(r.integral - ex) <= 2 * workload["epsrel"] * abs(ex))):
-            bad += 1
+        ok1 = r.status == 0 and (ex is None or abs(r.integral - ex) <= workload["epsrel"] * abs(ex))
+        ok2 = r.status == 0 and (ex is None or
+                                 abs(r.integral - ex) <= 2 * workload["epsrel"] * abs(ex))
+        bad += 0 if ok1 else 1
+        bad2 += 0 if ok2 else 1
     neval = sum(r.neval for r in results)
     nreg = {}
     for (fam, n), r in zip(fams, results):
@@ -546,37 +636,55 @@ def main() -> int:
         t = torch.tensor([dev_ms, wall], dtype=torch.float64, device="cuda")
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         dev_ms, wall = float(t[0]), float(t[1])
-        fb = torch.tensor([float(bad)], dtype=torch.float64, device="cuda")
+        fb = torch.tensor([float(bad), float(bad2)], dtype=torch.float64, device="cuda")
         pg.all_reduce(fb, op=pg.ReduceOp.SUM)
-        bad = int(fb[0])
-    value = world * nint * args.steps / (dev_ms / 1e3)
-    e2e_value = world * nint * args.steps / (wall / 1e3)
+        bad, bad2 = int(fb[0]), int(fb[1])
+    good = world * nint - bad
+    value = good * args.steps / (dev_ms / 1e3)
+    e2e_value = good * args.steps / (wall / 1e3)
 
     # roofline of the dominant kernel (FP64-bound rule evaluation).  The
     # regions are split between the persistent kernel (short lists) and the
     # multi-launch rule kernel (long lists); each gets its own share of the
     # algorithmic flops (per-region flops x regions it evaluated).
-    per_region = {k: flops_per_region(f, n) for (f, n) in nreg for k in [(f, n)]}
-    total_regions = sum(nreg.values()) * args.steps
-    mean_flops = sum(per_region[k] * c for k, c in nreg.items()) / max(1, sum(nreg.values()))
-    ml_regions = st["regions_evaluated"]
-    pk_regions = max(0, total_regions - ml_regions)
+    # Roofline of the dominant kernel (FP64-bound rule evaluation).  Each
+    # kernel gets the algorithmic flops of the regions it evaluated, per
+    # (family, ndim): the split of every integrand's regions between the
+    # persistent kernels and the multi-launch rule kernel is taken from one
+    # untimed pass with the counters read after each call (the split is the
+    # same every step).
+    persist_flops = ml_flops = p2_flops = 0.0
+    for (fam, n), (pk_r, ml_r, p2_r) in split.items():
+        persist_flops += pk_r * flops_per_region(fam, n) * args.steps
+        ml_flops += ml_r * flops_per_region(fam, n) * args.steps
+        p2_flops += p2_r * flops_per_region(fam, n) * args.steps
+    pk_name = "k_replicated" if st.get("replicated_launches", 0) >= max(
+        1, st["persistent_launches"] - st.get("replicated_launches", 0)) else "k_persistent"
     kernels = {
-        "k_persistent": (pk_regions * mean_flops, st["ms_persistent"]),
-        "k_eval": (ml_regions * mean_flops, st["ms_eval"]),
+        pk_name: (persist_flops, st["ms_persistent"]),
+        "k_eval": (ml_flops, st["ms_eval"]),
+        "k_phase2": (p2_flops, st["ms_phase2"]),
     }
     dom = max(kernels, key=lambda k: kernels[k][1])
     dom_flops, dom_ms = kernels[dom]
     achieved = dom_flops / (dom_ms / 1e3) / 1e12 if dom_ms > 0 else None
-    peak = measure_fp64_peak(torch) if rank == 0 else None
+    peak = cub.fp64_peak(local) if rank == 0 else None
+    peak_dgemm = measure_fp64_peak(torch) if rank == 0 else None
 
     cpu = None
     if rank == 0 and not args.no_cpu:
         per = sum(nreg.values()) / max(1, nint) if "tables" in workload else None
         rate, evr, cores, done, el = cpu_reference_rate(workload, args.cpu_seconds,
                                                         regions_per_integral=per)
+        rate1, _, _, done1, el1 = cpu_reference_rate(workload, args.cpu_seconds / 2, threads=1,
+                                                     regions_per_integral=per)
         cpu = {"value": rate, "unit": "integrals/s", "cores": cores, "kind": "port",
-               "sample": cpu_sample_text(workload, done, el, per)}
+               "sample": cpu_sample_text(workload, done, el, per), "cpu_model": cpu_model(),
+               "one_thread": {"value": rate1, "unit": "integrals/s", "cores": 1,
+                              "sample": cpu_sample_text(workload, done1, el1, per)}}
+    ref_gpu = None
+    if rank == 0 and not args.no_ref_gpu:
+        ref_gpu = reference_gpu_rate(workload, 3, max(5, args.steps), local)
 
     if rank == 0:
         line = {
@@ -590,27 +698,41 @@ def main() -> int:
                        "parallelism": ("replicas" if "items" in workload else
                                        f"shards{world}") if world > 1 else "single",
                        "l2": "flushed between steps (256 MB write)",
-                       "regions_per_step": int(sum(nreg.values()))},
+                       "regions_per_step": int(sum(nreg.values())),
+                       "timing": "value: CUDA events on the library's stream around each "
+                                 "step's public-API calls (inputs are parameter blocks; the "
+                                 "host drives the launches); e2e: host wall clock around "
+                                 "the same calls"},
             "geval_per_s": world * neval * args.steps / (dev_ms / 1e3) / 1e9,
             "e2e": {"value": e2e_value, "unit": "integrals/s",
                     "h2d_bytes_per_step": st.get("h2d_bytes", 0) // max(1, args.steps),
                     "d2h_bytes_per_step": st.get("d2h_bytes", 0) // max(1, args.steps)},
             "gpu_launches": st["launches"],
-            "roofline": {"kernel": dom, "bound": "tensor", "pipe": "fp64", "achieved": achieved,
-                         "peak": peak, "unit": "TFLOP/s",
+            "roofline": {"kernel": dom, "bound": "fp64", "pipe": "fp64 (CUDA cores)",
+                         "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": (achieved / peak) if achieved and peak else None,
                          "traffic": profiled_traffic(dom, args.workload),
-                         "peak_source": "in-run cuBLAS DGEMM 8192^3 on the FP64 tensor pipe (MEASURED_PEAKS.json has no FP64 figure)",
-                         "algorithmic_flops_per_region": mean_flops,
+                         "peak_source": "in-run DFMA throughput loop on the FP64 CUDA cores "
+                                        "(cub_fp64_peak); MEASURED_PEAKS.json has no FP64 figure",
+                         "peak_dgemm": peak_dgemm,
+                         "peak_dgemm_source": "in-run cuBLAS DGEMM 8192^3 (FP64 tensor path)",
                          "kernel_ms_per_step": {k: v[1] / args.steps for k, v in kernels.items()},
-                         "regions_per_step": {"k_persistent": pk_regions / args.steps,
-                                              "k_eval": ml_regions / args.steps},
+                         "algorithmic_flops_per_step": {k: v[0] / args.steps
+                                                        for k, v in kernels.items()},
+                         "regions_per_step": {pk_name: sum(v[0] for v in split.values()),
+                                              "k_eval": sum(v[1] for v in split.values()),
+                                              "k_phase2": sum(v[2] for v in split.values())},
                          "persistent_iterations_per_step": st["persistent_iterations"] / args.steps,
                          "eval_launches_per_step": st["eval_launches"] / args.steps},
             "cpu_baseline": cpu,
             "clocks": clocks.summary(),
-            "check": {"integrals": nint, "failed": bad},
+            "check": {"integrals": world * nint, "failed": bad, "failed_2epsrel": bad2,
+                      "rule": "status 0 and |I - I*| <= epsrel |I*| against the analytic or "
+                              "closed-form I*; value and e2e count only the integrals that "
+                              "pass (failed_2epsrel: the same test at 2 epsrel)"},
         }
+        if ref_gpu is not None:
+            line["reference_gpu"] = ref_gpu
         if plain_cmp is not None:
             line["plain_same_integrands"] = plain_cmp
         if single_cmp is not None:
@@ -624,8 +746,8 @@ def main() -> int:
         pg.barrier()
         pg.destroy_process_group()
     # integrals that miss the analytic value by more than 2 epsrel (or do not
-    # converge) are counted in "check"; the run itself succeeded
-    return 0
+    # converge) are counted in "check" and fail the run
+    return 1 if bad else 0
 
 
 if __name__ == "__main__":

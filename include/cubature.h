@@ -63,6 +63,11 @@ enum cub_policy {
 #define CUB_STATUS_OK 0 /* converged (reference errorFlag == 0)         */
 /* > 0: not converged; for the reference policy the number of failed
  * phase-2 boxes (GPUKernelquad.cu:891,910), for the breadth policy 1.  */
+/* The integrand returned a NaN or an infinite value: the integral stopped
+ * at the iteration whose sums met it (value and error are those sums).
+ * The reference does not detect this (a NaN region error fails no test
+ * there, GPUQuadPhases.cu:63-74, and its value enters the sum).          */
+#define CUB_STATUS_NONFINITE (1 << 30)
 
 /* Error codes (negative return values). */
 #define CUB_ERR_INVALID -1
@@ -105,6 +110,17 @@ typedef struct cub_options {
   int persistent_max_r;    /* most regions a block of the persistent kernel
                               evaluates at once (1, 2, 4 or 8; a region
                               gets 256/R threads); 0 = 8                  */
+  int no_replicated;       /* 1: batches of at most 32 integrals on short
+                              lists use the persistent kernel instead of
+                              the replicated-decision kernel (same
+                              results, bit for bit)                       */
+  long long barrier_spins; /* polls of a device-side grid barrier before
+                              it gives up (CUB_ERR_TIMEOUT); 0 = default
+                              (a few seconds)                             */
+  int test_hold_block;     /* failure-detection tests only: b + 1 keeps
+                              block b of the persistent kernels from
+                              arriving at their grid barriers, so every
+                              wait runs out; 0 = off                      */
 } cub_options;
 
 /* Library version, (major << 16) | minor. */
@@ -147,6 +163,10 @@ typedef struct cub_stats {
   double ms_persistent;       /* device time of the persistent kernel       */
   long long persistent_launches;
   long long persistent_iterations; /* iterations run inside it          */
+  long long replicated_launches; /* of those, launches of the replicated-
+                                    decision kernel (small batches)     */
+  long long persistent_regions;  /* regions evaluated by both persistent
+                                    kernels                             */
 } cub_stats;
 
 int cub_ctx_stats(const cub_ctx* ctx, cub_stats* out);
@@ -421,9 +441,10 @@ int cub_split(int ndim, long long n, const double* d_lo, const double* d_len, lo
  * CUB_ERR_INVALID).  The array is shared by every call on a device: calls
  * that overlap on the GPU race and must be serialised.  The first call on
  * each device looks up the array's address; make it before any stream
- * capture.  Same arguments and results as cub_split, minus the scratch.
- * No counterpart in the reference (its GenerateActiveIntervals mallocs and
- * frees its buffers on every iteration). */
+ * capture.  The address is kept for the process's lifetime: after a
+ * cudaDeviceReset of that device, the next call would use a stale address,
+ * so do not reset a device between calls.  Same arguments and results as
+ * cub_split, minus the scratch.  No counterpart in the reference. */
 int cub_split_noalloc(int ndim, long long n, const double* d_lo, const double* d_len,
                       long long ld, const int* d_active, const int* d_axis, double* d_out_lo,
                       double* d_out_len, long long out_ld, int layout, long long* d_count,
@@ -434,6 +455,13 @@ int cub_split_noalloc(int ndim, long long n, const double* d_lo, const double* d
  * [3] = sum err over active == 0.  Device output; fixed-order tree. */
 int cub_reduce(long long n, const double* d_avg, const double* d_err, const int* d_active,
                double* d_out, void* d_scratch, size_t scratch_bytes, void* stream);
+
+/* Measured FP64 throughput of the CUDA cores of `device` (DFMA loop,
+ * TFLOP/s, FMA = 2 flops) into *tflops: the roofline denominator of the
+ * rule kernels, whose FP64 work is DFMA/DMUL/DADD on the CUDA cores.  A
+ * measurement utility with no counterpart in the reference; it launches on
+ * the device's legacy default stream and waits for it. */
+int cub_fp64_peak(int device, double* tflops);
 
 #ifdef __cplusplus
 }

@@ -22,6 +22,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -30,6 +31,7 @@
 #include "engine_kernels.cuh"
 #include "persistent.cuh"
 #include "phase2_kernels.cuh"
+#include "replicated.cuh"
 #include "rule9.hpp"
 
 namespace cubature {
@@ -44,6 +46,9 @@ struct Options {
   int persistent = 1;             // use the persistent kernel for short lists
   int persistent_max_n = 0;       // list length where it hands over; 0 auto
   int persistent_max_r = 0;       // most regions per block in the persistent kernel (1,2,4,8); 0 = 8
+  int replicated = 1;             // small batches: the replicated-decision kernel for short lists
+  long long barrier_spins = 0;    // grid-barrier polls before a timeout; 0 = kBarrierSpins
+  int hold_block = -1;            // tests: this block never arrives at a grid barrier
 };
 
 struct Result {
@@ -80,6 +85,8 @@ struct Stats {
   double ms_persistent = 0;      // device time of the persistent kernel (timing on)
   long long persistent_launches = 0;
   long long persistent_iterations = 0;
+  long long replicated_launches = 0;  // persistent launches of the replicated kernel
+  long long persistent_regions = 0;   // regions evaluated by both persistent kernels
 };
 
 inline const char* state_name(int s) {
@@ -123,6 +130,7 @@ class Workspace {
     part = nullptr;
     chunk_cnt = int_cnt = nullptr;
     axis_alt = excl_alt = chunk_int = nullptr;
+    avg_alt = err_alt = nullptr;
     cmask = nullptr;
     box = nullptr;
     box_cap_ = 0;
@@ -165,6 +173,9 @@ class Workspace {
   // second parity of the persistent kernel's lazy split
   int* axis_alt = nullptr;
   int* excl_alt = nullptr;
+  // second parity of the replicated kernel's per-slot values and errors
+  double* avg_alt = nullptr;
+  double* err_alt = nullptr;
   unsigned* cmask = nullptr;  // two arrays of nchunk masks
   int* chunk_int = nullptr;
   double* box = nullptr;  // integration boxes of the current batch
@@ -260,7 +271,8 @@ class Workspace {
         !alloc(&part, sizeof(ChunkPartial) * nchunk) || !alloc(&chunk_excl, sizeof(int) * nchunk) ||
         !alloc(&chunk_cnt, sizeof(unsigned) * nchunk) || !alloc(&axis_alt, sizeof(int) * ncap) ||
         !alloc(&excl_alt, sizeof(int) * nchunk) || !alloc(&cmask, sizeof(unsigned) * 2 * nchunk) ||
-        !alloc(&chunk_int, sizeof(int) * nchunk))
+        !alloc(&chunk_int, sizeof(int) * nchunk) || !alloc(&avg_alt, sizeof(double) * ncap) ||
+        !alloc(&err_alt, sizeof(double) * ncap))
       return false;
     if (!ck(cudaMemsetAsync(chunk_cnt, 0, sizeof(unsigned) * nchunk, s))) return false;
     cap_ = ncap;
@@ -346,6 +358,8 @@ class Workspace {
     free_buf(excl_alt);
     free_buf(cmask);
     free_buf(chunk_int);
+    free_buf(avg_alt);
+    free_buf(err_alt);
   }
 
   bool reserve_integrals(int nint, cudaStream_t s) {
@@ -530,22 +544,37 @@ inline void state_results(const IntegralState* h, int nint, Result* out) {
   }
 }
 
+// Blocks per SM of a cooperative launch of `kernel` (256 threads), cached
+// per device and kernel instantiation in `cache` (0: not yet queried,
+// else 1 + blocks per SM, or 1 when the device has no cooperative launch).
+// The query is idempotent, so concurrent first calls from several host
+// threads store the same value.
+inline int coop_blocks(std::atomic<int>* cache, int device, const void* kernel, int sms) {
+  const int dev = device & 63;
+  int v = cache[dev].load(std::memory_order_relaxed);
+  if (v == 0) {
+    int per_sm = 0, coop = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, 0);
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device);
+    v = 1 + (coop ? per_sm : 0);
+    cache[dev].store(v, std::memory_order_relaxed);
+  }
+  return (v - 1) * sms;
+}
+
 // Blocks of a cooperative k_persistent<N, Src> launch on the workspace's
-// device (queried once per device and instantiation); 0 when the device
-// has no cooperative launch.
+// device; 0 when the device has no cooperative launch.
 template <int N, class Src>
 int persistent_blocks(const Workspace& ws, int sms) {
-  static int per_sm_cache[64];
-  static bool cached[64];
-  const int dev = ws.device() & 63;
-  if (!cached[dev]) {
-    int per_sm = 0, coop = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_persistent<N, Src>, 256, 0);
-    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, ws.device());
-    per_sm_cache[dev] = coop ? per_sm : 0;
-    cached[dev] = true;
-  }
-  return per_sm_cache[dev] > 0 ? per_sm_cache[dev] * sms : 0;
+  static std::atomic<int> cache[64];
+  return coop_blocks(cache, ws.device(), (const void*)k_persistent<N, Src>, sms);
+}
+
+// The same for k_replicated<N, Src>.
+template <int N, class Src>
+int replicated_blocks(const Workspace& ws, int sms) {
+  static std::atomic<int> cache[64];
+  return coop_blocks(cache, ws.device(), (const void*)k_replicated<N, Src>, sms);
 }
 
 // Longest list a persistent launch keeps iterating on.
@@ -620,7 +649,47 @@ inline PersistArgs persist_args(const Workspace& ws, const EngineArgs& a, const 
   p.box = d_box;
   p.host_out = nullptr;
   p.host_words = 0;
+  p.spin_limit = opt.barrier_spins > 0 ? opt.barrier_spins : detail::kBarrierSpins;
+  p.hold_block = opt.hold_block;
   return p;
+}
+
+// Arguments of a replicated-kernel launch over the lists bound in `a`.
+inline RepArgs rep_args(const Workspace& ws, const EngineArgs& a, const Options& opt,
+                        int iter_base, int rmax, bool init, int dv, int per, int padded,
+                        const double* d_box) {
+  RepArgs p;
+  p.base = a;
+  for (int b = 0; b < 2; ++b) {
+    p.lo[b] = ws.lo[b];
+    p.len[b] = ws.len[b];
+    p.rid[b] = ws.rid[b];
+  }
+  p.avg[0] = ws.avg;
+  p.avg[1] = ws.avg_alt;
+  p.err[0] = ws.err;
+  p.err[1] = ws.err_alt;
+  p.axis[0] = ws.axis;
+  p.axis[1] = ws.axis_alt;
+  p.max_n = rmax;
+  p.max_r = opt.persistent_max_r > 0 ? opt.persistent_max_r : 8;
+  p.iter_base = iter_base;
+  p.init = init ? 1 : 0;
+  p.divisions = dv;
+  p.per_integral = per;
+  p.padded = padded;
+  p.box = d_box;
+  p.host_out = nullptr;
+  p.host_words = 0;
+  p.spin_limit = opt.barrier_spins > 0 ? opt.barrier_spins : detail::kBarrierSpins;
+  p.hold_block = opt.hold_block;
+  return p;
+}
+
+// Longest list a replicated launch evaluates.
+inline int replicated_limit(const Options& opt, int rblocks) {
+  return std::min(opt.persistent_max_n > 0 ? opt.persistent_max_n : rblocks * 8,
+                  32 * kRepChunks);
 }
 
 // Pinned control block for a persistent launch starting from `hs`.
@@ -701,10 +770,18 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
   const int pblocks =
       opt.persistent && !Hook::kActive ? detail::persistent_blocks<N, Src>(ws, sms) : 0;
   const int pmax = detail::persistent_limit(opt, pblocks);
+  const int rblocks = opt.persistent && opt.replicated && !Hook::kActive && nint <= kSmallBatch
+                          ? detail::replicated_blocks<N, Src>(ws, sms)
+                          : 0;
+  const int rmax = detail::replicated_limit(opt, rblocks);
 
   IterState hs = c0.host;
   long long n_left = 0;
   bool states_fresh = true;  // h holds the device states after the last kernel
+  // regions of each integral before a persistent launch (statistics)
+  unsigned long long nreg_small[kSmallBatch];
+  std::vector<unsigned long long> nreg_big(nint > kSmallBatch ? nint : 0);
+  unsigned long long* nreg_before = nint > kSmallBatch ? nreg_big.data() : nreg_small;
   int status = kOk;
   while (hs.n_running > 0 && hs.n > 0) {
     n_cur = hs.n;
@@ -723,32 +800,65 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
       return kErrCuda;
     bind(n_cur);
 
-    if (pblocks > 0 && n_cur <= pmax) {
-      // a stretch of iterations in one persistent launch
+    const bool use_rep = rblocks > 0 && n_cur <= rmax;
+    if (use_rep || (pblocks > 0 && n_cur <= pmax)) {
+      // a stretch of iterations in one persistent launch: the
+      // replicated-decision kernel for small batches on short lists, else
+      // the persistent kernel
       detail::persistent_control(ws, hs, cur);
-      const size_t up = uploaded ? sizeof(Control) : ws.state_bytes(nint);
+      // the replicated kernel reads the states every launch (its blocks
+      // keep their own copies); the persistent kernel keeps them on the
+      // device between its launches
+      const size_t up = uploaded && !use_rep ? sizeof(Control) : ws.state_bytes(nint);
+      if (use_rep && uploaded && !states_fresh) {
+        // the device holds the newer states (multi-launch steps ran since
+        // the last copy back): fetch them before re-uploading
+        if (!ws.ck(cudaMemcpyAsync(ws.ist_host_, ws.ist, sizeof(IntegralState) * nint,
+                                   cudaMemcpyDeviceToHost, s)) ||
+            !ws.ck(cudaStreamSynchronize(s)))
+          return kErrCuda;
+        st.d2h_bytes += (long long)(sizeof(IntegralState) * nint);
+        detail::persistent_control(ws, hs, cur);
+      }
       if (!ws.ck(cudaMemcpyAsync(ws.ctl, ws.ctl_host_, up, cudaMemcpyHostToDevice, s)))
         return kErrCuda;
       uploaded = true;
       st.h2d_bytes += (long long)up;
-      PersistArgs p = detail::persist_args(ws, a, opt, c0.iters_done, pmax, grid_pending, dv,
-                                           per, padded, d_box);
-      p.host_out = ws.direct_states(nint);
-      p.host_words = (int)(ws.state_bytes(nint) / 8);
-      grid_pending = false;
-      void* args[] = {(void*)&src, (void*)&T, (void*)&p};
+      // the host copy of the states is current unless multi-launch steps ran
+      // since it was read (the replicated path fetched it above)
+      const bool count_regions = use_rep || states_fresh;
+      if (count_regions)
+        for (int k = 0; k < nint; ++k) nreg_before[k] = h[k].nregions;
       if (ws.timing) ws.ck(cudaEventRecord(ws.ev[0], s));
-      if (!ws.ck(cudaLaunchCooperativeKernel((const void*)k_persistent<N, Src>, dim3(pblocks),
-                                             dim3(256), args, 0, s)))
-        return kErrCuda;
+      if (use_rep) {
+        RepArgs p = detail::rep_args(ws, a, opt, c0.iters_done, rmax, grid_pending, dv, per,
+                                     padded, d_box);
+        p.host_out = ws.direct_states(nint);
+        p.host_words = (int)(ws.state_bytes(nint) / 8);
+        void* args[] = {(void*)&src, (void*)&T, (void*)&p};
+        if (!ws.ck(cudaLaunchCooperativeKernel((const void*)k_replicated<N, Src>,
+                                               dim3(rblocks), dim3(256), args, 0, s)))
+          return kErrCuda;
+      } else {
+        PersistArgs p = detail::persist_args(ws, a, opt, c0.iters_done, pmax, grid_pending, dv,
+                                             per, padded, d_box);
+        p.host_out = ws.direct_states(nint);
+        p.host_words = (int)(ws.state_bytes(nint) / 8);
+        void* args[] = {(void*)&src, (void*)&T, (void*)&p};
+        if (!ws.ck(cudaLaunchCooperativeKernel((const void*)k_persistent<N, Src>,
+                                               dim3(pblocks), dim3(256), args, 0, s)))
+          return kErrCuda;
+      }
+      grid_pending = false;
       if (ws.timing) ws.ck(cudaEventRecord(ws.ev[1], s));
       st.launches += 1;
       st.persistent_launches += 1;
       // the states come back with the control block (stored by the kernel
       // itself for small batches): when the launch finished every
       // integral, no further round trip is needed
-      if (!p.host_out && !ws.ck(cudaMemcpyAsync(ws.ctl_host_, ws.ctl, ws.state_bytes(nint),
-                                                cudaMemcpyDeviceToHost, s)))
+      if (!ws.direct_states(nint) &&
+          !ws.ck(cudaMemcpyAsync(ws.ctl_host_, ws.ctl, ws.state_bytes(nint),
+                                 cudaMemcpyDeviceToHost, s)))
         return kErrCuda;
       if (!ws.ck(cudaStreamSynchronize(s))) return kErrCuda;
       st.d2h_bytes += (long long)ws.state_bytes(nint);
@@ -762,6 +872,10 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
       const int before = c0.iters_done;
       st.iterations += c.iters_done - before;
       st.persistent_iterations += c.iters_done - before;
+      if (use_rep) st.replicated_launches += 1;
+      if (count_regions)
+        for (int k = 0; k < nint; ++k)
+          st.persistent_regions += (long long)(h[k].nregions - nreg_before[k]);
       c0.iters_done = c.iters_done;
       if (c.exit_reason == kExitTimeout || c.timeout) {
         ws.ck(cudaErrorLaunchTimeout);

@@ -35,6 +35,10 @@ namespace cubature {
 
 enum Policy : int { kPolicyReference = 0, kPolicyBreadth = 1 };
 
+// Status of an integral whose sums stopped being finite (a NaN or infinite
+// integrand value), CUB_STATUS_NONFINITE of the C ABI.
+constexpr int kStatusNonFinite = 1 << 30;
+
 enum IntegralStateCode : int {
   kStateRunning = 0,
   kStateDone = 1,      // converged or out of active regions
@@ -88,11 +92,15 @@ struct Control {
   unsigned bar_count;  // grid barrier arrivals since the launch (monotonic)
   unsigned bar_gen;    // unused
   int timeout;         // a bounded wait gave up
-  // globaltimer stamps (ns) of the persistent kernel's first kTraceIters
+  // globaltimer stamps (ns) of the persistent kernels' first kTraceIters
   // iterations, kTraceSlots per iteration (diagnostics, read back with the
-  // control block): 0 start, 1 next list assigned, 2 grid barrier passed,
-  // 3 decider read its integral state, 4 block 0's evaluations done, 5 last
-  // chunk summed, 6 integrals decided, 7 chunk sums combined
+  // control block).  Persistent kernel: 0 start, 1 next list assigned,
+  // 2 grid barrier passed, 3 decider read its integral state, 4 block 0's
+  // evaluations done, 5 last chunk summed, 6 integrals decided, 7 chunk sums
+  // combined.  Replicated kernel (block 0): 0 start, 7 first region set up,
+  // 4 evaluations done, 2 grid barrier passed, 1 chunk owners found,
+  // 3 chunk partials formed, 5 integrals decided (warp 0), 6 decision
+  // visible to the block.
   unsigned long long trace[64];
 };
 constexpr int kTraceIters = 8;
@@ -272,7 +280,13 @@ __device__ __forceinline__ void decide_integral(IntegralState& is, double s0, do
   is.iters += 1;
   is.next_count = 0;
   is.left_new = 0;
-  if (errG <= max_err(rG, is.epsrel, is.epsabs)) {
+  if (!isfinite(s0) || !isfinite(s1)) {
+    // a NaN or infinite integrand value reached the sums: stop here
+    is.value = rG;
+    is.error = errG;
+    is.state = kStateDone;
+    is.status = kStatusNonFinite;
+  } else if (errG <= max_err(rG, is.epsrel, is.epsabs)) {
     // global stop test (GPUKernelquad.cu:583-598)
     is.value = rG;
     is.error = errG;

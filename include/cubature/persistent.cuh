@@ -65,6 +65,8 @@ struct PersistArgs {
   // and the host needs no copy back.
   Control* host_out;
   int host_words;
+  long long spin_limit;  // grid-barrier polls before giving up
+  int hold_block;        // failure-detection tests: this block never arrives (-1: none)
 };
 
 // How the first step of an iteration obtains a slot's region.
@@ -89,21 +91,24 @@ __device__ __forceinline__ void red_release_add(unsigned* p, unsigned v) {
 }
 
 // Grid-wide barrier on a monotonic arrival counter: the b-th barrier of a
-// launch (b = 1, 2, ...) waits for b * gridDim.x arrivals.  Bounded wait;
-// returns false once any block gave up waiting (all blocks then return).
+// launch (b = 1, 2, ...) waits for b * gridDim.x arrivals.  Bounded wait
+// (spin_limit polls); returns false once any block gave up waiting (all
+// blocks then return).  A block with arrive == false waits without
+// arriving: the failure-detection tests use it to make every wait run out.
 // Ordering needs no separate fences: the block's writes precede thread 0's
 // gpu-scope release through the CTA barrier, the release and acquire
 // operations are cumulative, and the closing CTA barrier orders the
 // block's later reads after thread 0's acquire.
-__device__ __forceinline__ bool grid_barrier(Control* ctl, unsigned target) {
+__device__ __forceinline__ bool grid_barrier(Control* ctl, unsigned target, long long spin_limit,
+                                             bool arrive) {
   __shared__ int ok;
   __syncthreads();
   if (threadIdx.x == 0) {
-    red_release_add(&ctl->bar_count, 1u);
+    if (arrive) red_release_add(&ctl->bar_count, 1u);
     long long spins = 0;
     int good = 1;
     while (ld_acquire(&ctl->bar_count) < target) {
-      if (++spins > kBarrierSpins || *(volatile int*)&ctl->timeout) {
+      if (++spins > spin_limit || *(volatile int*)&ctl->timeout) {
         atomicExch(&ctl->timeout, 1);
         good = 0;
         break;
@@ -248,58 +253,32 @@ struct GroupSmem {
   int owner[8];
 };
 
-// Barrier for the groups of a block.  All groups of a block step through
-// their slots in lockstep (eval_step), so a block-wide barrier serves every
-// group size and no named barriers are needed.
-template <int G>
-__device__ __forceinline__ void group_sync(int) {
-  __syncthreads();
-}
-
-// One region evaluated by the G threads of group g, one point per thread
-// per round.  Thread 0 of the group returns the result.  Every thread of
-// the block must call it (it contains block barriers); groups with
-// active == false evaluate nothing.
-template <int N, int G, class F>
-__device__ __forceinline__ RegionResult eval_region_group(const F& f, const double (&L)[N],
-                                                          const double (&H)[N], const RuleTables& T,
-                                                          GroupSmem<N>& sm, int g, int t,
-                                                          bool active) {
+// The set sums of the G threads of a group (S, per thread) combined into
+// the region's result: warp shuffle trees, then the warps' partials in
+// warp order; the fourth difference per axis from the staged centre and
+// set-1/2 values (fst); value, error and split axis (finish_region).
+// Thread 0 of the group returns the result.  Every thread of the block must
+// call it (block barriers).
+// A set whose sums are +0.0 in every lane of a warp reduces to +0.0, so
+// its shuffle tree is skipped (same bits).
+template <int N, int G>
+__device__ __forceinline__ RegionResult group_finish(double (&S)[kNumSets], const double (&H)[N],
+                                                     const RuleTables& T,
+                                                     double (&red)[8][kNumSets], const double* fst,
+                                                     int t) {
   constexpr int W = G / 32;
   const int lane = t & 31, wid = threadIdx.x >> 5;
-  double S[kNumSets];
-#pragma unroll
-  for (int k = 0; k < kNumSets; ++k) S[k] = 0;
-  // Branch-free body, two points in flight per thread.  A thread's points
-  // of one set are consecutive, so adding into S[set] directly gives the
-  // same sums as a running sum flushed at set changes.
-  const int p0 = active ? t : PointTable<N>::kPoints;
-  auto point = [&](int p) {
-    const uint2 e = sm.pt.ent[p];
-    double x[N];
-#pragma unroll
-    for (int i = 0; i < N; ++i) x[i] = fma(sm.pt.ctab[(e.x >> (4 * i)) & 15u], H[i], L[i]);
-    const double fx = call_point(f, x, p);
-    if (p <= 4 * N) sm.fstage[g][p] = fx;
-#pragma unroll
-    for (int k = 0; k < kNumSets; ++k) S[k] += (e.y == (unsigned)k) ? fx : 0.0;
-  };
-  if constexpr (kTwoPointsInFlight<F>) {
-#pragma unroll 2
-    for (int p = p0; p < PointTable<N>::kPoints; p += G) point(p);
-  } else {
-#pragma unroll 1
-    for (int p = p0; p < PointTable<N>::kPoints; p += G) point(p);
-  }
 #pragma unroll
   for (int k = 0; k < kNumSets; ++k) {
     double v = S[k];
+    if (__any_sync(0xffffffffu, __double_as_longlong(v) != 0)) {
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+      for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    }
     S[k] = v;
-    if (W > 1 && lane == 0) sm.red[wid][k] = v;
+    if (W > 1 && lane == 0) red[wid][k] = v;
   }
-  group_sync<G>(g);
+  __syncthreads();
   RegionResult r;
   r.avg = r.err = 0;
   r.axis = 0;
@@ -309,7 +288,7 @@ __device__ __forceinline__ RegionResult eval_region_group(const F& f, const doub
     for (int k = 0; k < kNumSets; ++k) {
       if (W > 1) {
         double v = 0;
-        for (int w = 0; w < W; ++w) v += sm.red[wid + w][k];
+        for (int w = 0; w < W; ++w) v += red[wid + w][k];
         rs.S[k] = v;
       } else {
         rs.S[k] = S[k];
@@ -319,7 +298,7 @@ __device__ __forceinline__ RegionResult eval_region_group(const F& f, const doub
     rs.best = 0;
     rs.axis = -1;
     if (lane < N) {
-      const double* fs = sm.fstage[g];
+      const double* fs = fst;
       const double ratio = T.ratio;
       const double base = __dmul_rn(__dmul_rn(fs[0], 2.0), __dadd_rn(1.0, -ratio));
       const int d = lane;
@@ -344,8 +323,44 @@ __device__ __forceinline__ RegionResult eval_region_group(const F& f, const doub
       r = finish_region<N>(rs, T, jac, 0);
     }
   }
-  group_sync<G>(g);
+  __syncthreads();
   return r;
+}
+
+// One region evaluated by the G threads of group g, one point per thread
+// per round.  Thread 0 of the group returns the result.  Every thread of
+// the block must call it (it contains block barriers); groups with
+// active == false evaluate nothing.
+template <int N, int G, class F>
+__device__ __forceinline__ RegionResult eval_region_group(const F& f, const double (&L)[N],
+                                                          const double (&H)[N], const RuleTables& T,
+                                                          GroupSmem<N>& sm, int g, int t,
+                                                          bool active) {
+  double S[kNumSets];
+#pragma unroll
+  for (int k = 0; k < kNumSets; ++k) S[k] = 0;
+  // Branch-free body, two points in flight per thread.  A thread's points
+  // of one set are consecutive, so adding into S[set] directly gives the
+  // same sums as a running sum flushed at set changes.
+  const int p0 = active ? t : PointTable<N>::kPoints;
+  auto point = [&](int p) {
+    const uint2 e = sm.pt.ent[p];
+    double x[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) x[i] = fma(sm.pt.ctab[(e.x >> (4 * i)) & 15u], H[i], L[i]);
+    const double fx = call_point(f, x, p);
+    if (p <= 4 * N) sm.fstage[g][p] = fx;
+#pragma unroll
+    for (int k = 0; k < kNumSets; ++k) S[k] += (e.y == (unsigned)k) ? fx : 0.0;
+  };
+  if constexpr (kTwoPointsInFlight<F>) {
+#pragma unroll 2
+    for (int p = p0; p < PointTable<N>::kPoints; p += G) point(p);
+  } else {
+#pragma unroll 1
+    for (int p = p0; p < PointTable<N>::kPoints; p += G) point(p);
+  }
+  return group_finish<N, G>(S, H, T, sm.red, sm.fstage[g], t);
 }
 
 // atomicAdd with acquire-release semantics at GPU scope: publishes the
@@ -1020,7 +1035,8 @@ __global__ void __launch_bounds__(256, 2) k_persistent(Src src, RuleTables T, Pe
     }
     if (tracer) trace_mark(ctl, it, 4);
     ++barriers;
-    if (!detail::grid_barrier(ctl, barriers * gridDim.x)) {
+    if (!detail::grid_barrier(ctl, barriers * gridDim.x, p.spin_limit,
+                              (int)blockIdx.x != p.hold_block)) {
       reason = kExitTimeout;
       break;
     }

@@ -293,6 +293,7 @@ static __global__ void k_phase2_collect(IntegralState* ist, int nint, const Left
       is.neval += (nr - n) * (unsigned long long)npoints * 2ull + n * (unsigned long long)npoints;
       is.status = nf;
       if (is.error <= detail::max_err(is.value, is.epsrel, is.epsabs)) is.status = 0;
+      if (!isfinite(v) || !isfinite(e)) is.status = kStatusNonFinite;
       is.state = kStateDone;
     }
   }

@@ -54,6 +54,7 @@ def _stale(obj: Path, src: Path, deps: list[Path]) -> bool:
 def units() -> list[tuple[Path, Path, list[str]]]:
     out = [(CSRC / "capi.cu", OBJ / "capi.o", []),
            (CSRC / "noalloc.cu", OBJ / "noalloc.o", []),
+           (CSRC / "peak.cu", OBJ / "peak.o", []),
            (CSRC / "capi_tables.cu", OBJ / "capi_tables.o", []),
            (CSRC / "graph.cu", OBJ / "graph.o", []),
            (CSRC / "mlp.cu", OBJ / "mlp.o", [])]

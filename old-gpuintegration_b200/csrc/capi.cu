@@ -67,6 +67,9 @@ Options to_options(const cub_options* opt) {
   o.persistent = opt->no_persistent ? 0 : 1;
   if (opt->persistent_max_n > 0) o.persistent_max_n = opt->persistent_max_n;
   if (opt->persistent_max_r > 0) o.persistent_max_r = opt->persistent_max_r;
+  o.replicated = opt->no_replicated ? 0 : 1;
+  if (opt->barrier_spins > 0) o.barrier_spins = opt->barrier_spins;
+  o.hold_block = opt->test_hold_block > 0 ? opt->test_hold_block - 1 : -1;
   return o;
 }
 
@@ -146,6 +149,9 @@ void cub_default_options(cub_options* opt) {
   opt->no_persistent = o.persistent ? 0 : 1;
   opt->persistent_max_n = o.persistent_max_n;
   opt->persistent_max_r = o.persistent_max_r;
+  opt->no_replicated = o.replicated ? 0 : 1;
+  opt->barrier_spins = 0;
+  opt->test_hold_block = 0;
 }
 
 cub_ctx* cub_create(int device) {
@@ -208,6 +214,8 @@ int cub_ctx_stats(const cub_ctx* ctx, cub_stats* out) {
   out->ms_persistent = s.ms_persistent;
   out->persistent_launches = s.persistent_launches;
   out->persistent_iterations = s.persistent_iterations;
+  out->replicated_launches = s.replicated_launches;
+  out->persistent_regions = s.persistent_regions;
   return 0;
 }
 

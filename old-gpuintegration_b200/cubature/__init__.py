@@ -81,6 +81,8 @@ class CStats(C.Structure):
         ("ms_persistent", C.c_double),
         ("persistent_launches", C.c_longlong),
         ("persistent_iterations", C.c_longlong),
+        ("replicated_launches", C.c_longlong),
+        ("persistent_regions", C.c_longlong),
     ]
 
     def as_dict(self) -> dict:
@@ -98,6 +100,9 @@ class COptions(C.Structure):
         ("no_persistent", C.c_int),
         ("persistent_max_n", C.c_int),
         ("persistent_max_r", C.c_int),
+        ("no_replicated", C.c_int),
+        ("barrier_spins", C.c_longlong),
+        ("test_hold_block", C.c_int),
     ]
 
 
@@ -129,7 +134,7 @@ EXPORTS = (
     "cub_mlp_set_data", "cub_mlp_params", "cub_mlp_grad", "cub_mlp_train", "cub_mlp_eval",
     "cub_cv_default_options", "cub_cv_integrate_batch", "cub_autotune_batch",
     "cub_integrate_mixed_batch", "cub_graph_create", "cub_graph_launch", "cub_graph_info",
-    "cub_graph_destroy",
+    "cub_graph_destroy", "cub_fp64_peak",
 )
 
 _lib = None
@@ -214,9 +219,17 @@ def load_library(path: str | Path | None = None):
     L.cub_reduce.argtypes = [C.c_longlong, vp, vp, vp, vp, vp, C.c_size_t, vp]
     L.cub_split_noalloc.argtypes = [C.c_int, C.c_longlong, vp, vp, C.c_longlong, vp, vp, vp, vp,
                                     C.c_longlong, C.c_int, vp, vp]
+    L.cub_fp64_peak.argtypes = [C.c_int, dp]
     if path is None:
         _lib = L
     return L
+
+
+def fp64_peak(device: int = 0) -> float:
+    """FP64 CUDA-core throughput of `device` in TFLOP/s (cub_fp64_peak)."""
+    out = C.c_double()
+    _check(load_library().cub_fp64_peak(device, C.byref(out)))
+    return out.value
 
 
 def last_error() -> str:
@@ -290,7 +303,8 @@ class Result:
 def options(policy: int = POLICY_REFERENCE, phase1_cap: int = 0, max_iters: int = 0,
             phase2_max_regions: int = 0, max_slots: int = 0, lanes: int = 0,
             persistent: bool = True, persistent_max_n: int = 0,
-            persistent_max_r: int = 0) -> COptions:
+            persistent_max_r: int = 0, replicated: bool = True, barrier_spins: int = 0,
+            test_hold_block: int = -1) -> COptions:
     o = COptions()
     load_library().cub_default_options(C.byref(o))
     o.policy = policy
@@ -308,6 +322,9 @@ def options(policy: int = POLICY_REFERENCE, phase1_cap: int = 0, max_iters: int 
         o.persistent_max_n = persistent_max_n
     if persistent_max_r:
         o.persistent_max_r = persistent_max_r
+    o.no_replicated = 0 if replicated else 1
+    o.barrier_spins = barrier_spins
+    o.test_hold_block = test_hold_block + 1 if test_hold_block >= 0 else 0
     return o
 
 

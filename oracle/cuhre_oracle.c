@@ -801,7 +801,7 @@ int orc_integrate_reference(const orc_rule* r, const orc_integrand* f, double ep
 
   double integral = 0, error = 0;
   size_t nregions = 0, neval = 0;
-  int iters = 0;
+  int iters = 0, nonfinite = 0;
   for (int it = 0; it < 100; ++it) {
     double* avg = (double*)malloc(sizeof(double) * n);
     double* err = (double*)malloc(sizeof(double) * n);
@@ -819,6 +819,15 @@ int orc_integrate_reference(const orc_rule* r, const orc_integrand* f, double ep
     double rG = integral + sum_avg, errG = error + sum_err;
     integral += fin_avg;
     error += fin_err;
+    if (!isfinite(sum_avg) || !isfinite(sum_err)) {
+      /* a NaN or infinite integrand value: stop with the sums as they are */
+      integral = rG;
+      error = errG;
+      nonfinite = 1;
+      n = 0;
+      free(avg); free(err); free(axis); free(act);
+      break;
+    }
     if (errG <= max_err(rG, epsrel, epsabs)) {
       integral = rG;
       error = errG;
@@ -860,7 +869,11 @@ int orc_integrate_reference(const orc_rule* r, const orc_integrand* f, double ep
       cnt[i] = orc_phase2_box(r, f, L, W, epsrel, epsabs, phase2_max, &res[i], &er[i], &fail[i]);
     }
     size_t total = 0, failed = 0;
-    for (size_t i = 0; i < n; ++i) { total += (size_t)cnt[i]; failed += (size_t)fail[i]; }
+    for (size_t i = 0; i < n; ++i) {
+      total += (size_t)cnt[i];
+      failed += (size_t)fail[i];
+      if (!isfinite(res[i]) || !isfinite(er[i])) nonfinite = 1;
+    }
     integral += psum(res, n);
     error += psum(er, n);
     nregions += total;
@@ -870,6 +883,7 @@ int orc_integrate_reference(const orc_rule* r, const orc_integrand* f, double ep
     free(res); free(er); free(cnt); free(fail);
   }
   if (error <= max_err(integral, epsrel, epsabs)) status = 0;
+  if (nonfinite) status = ORC_STATUS_NONFINITE;
   free(lo);
   free(len);
   out->value = integral;

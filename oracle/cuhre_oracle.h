@@ -28,6 +28,10 @@ extern "C" {
 #define ORC_MAXDIM 16
 #define ORC_NSETS 9
 #define ORC_NRULES 5
+/* Status of an integral whose integrand gave a NaN or an infinite value:
+ * the value and error sums stopped being finite (an extension of the
+ * engine, which the reference does not detect). */
+#define ORC_STATUS_NONFINITE (1 << 30)
 
 /* Integrand families.  The numbering is shared with include/cubature.h. */
 enum {

@@ -371,3 +371,58 @@ def make_table7(spline_x, spline_y, grid_x, grid_y, grid_z, sigma, offset) -> In
     f.tables = C.cast(C.pointer(T), C.c_void_p)
     f._keep = (T, sp, gr)
     return f
+
+
+# -- closed-form value of the 7-D table integrand ----------------------------
+def _gauss_legendre(a: float, b: float, n: int):
+    x, w = np.polynomial.legendre.leggauss(n)
+    return 0.5 * (b - a) * x + 0.5 * (b + a), 0.5 * (b - a) * w
+
+
+def table7_exact(spline_x, spline_y, grid_x, grid_y, grid_z, sigma, offset, y2=None) -> float:
+    """Integral over [0,1]^7 of spline(x0) * bilinear(x1, x2) *
+    exp(-(4 x3 - mu)^2 / (2 sigma^2)), mu = offset + 2 x4 + 0.1 (x5 + x6),
+    to FP64 rounding, for knots that span [0, 1] on every table axis.
+
+    The integrand factorises.  The natural cubic spline integrates cell by
+    cell in closed form, h (y_i + y_i+1) / 2 - h^3 (y2_i + y2_i+1) / 24; the
+    bilinear interpolant integrates exactly by the trapezoid rule on its
+    grid.  For the kernel, with k = 1 / (sigma sqrt 2) and
+    c = offset + 2 x4 + 0.1 s, s = x5 + x6: the x3 integral is
+    sqrt(pi) / (8 k) (erf(k (4 - c)) + erf(k c)); the x4 integral follows
+    from the antiderivative A(c) = c erf(k c) + exp(-k^2 c^2) / (k sqrt pi)
+    of erf(k c); the s integral, with the density 1 - |s - 1| of x5 + x6 on
+    [0, 2], is a 48-point Gauss-Legendre rule on each side of the kink at
+    s = 1 (the integrand in s is entire and varies on a scale of ~3 in s).
+    """
+    from math import erf, exp, pi, sqrt
+
+    sx, sy = _f64(spline_x), _f64(spline_y)
+    if abs(sx[0]) > 0 or abs(sx[-1] - 1.0) > 0:
+        raise ValueError("spline knots must span [0, 1]")
+    y2 = spline_second_derivs(sx, sy) if y2 is None else _f64(y2)
+    h = np.diff(sx)
+    spline_int = float(np.sum(h * (sy[:-1] + sy[1:]) / 2 - h ** 3 * (y2[:-1] + y2[1:]) / 24))
+
+    gx, gy = _f64(grid_x), _f64(grid_y)
+    gz = _f64(grid_z).reshape(len(gx), len(gy))
+    if gx[0] != 0 or gx[-1] != 1 or gy[0] != 0 or gy[-1] != 1:
+        raise ValueError("grid knots must span [0, 1]^2")
+    cell = np.outer(np.diff(gx), np.diff(gy)) / 4
+    grid_int = float(np.sum(cell * (gz[:-1, :-1] + gz[1:, :-1] + gz[:-1, 1:] + gz[1:, 1:])))
+
+    k = 1.0 / (float(sigma) * sqrt(2.0))
+
+    def anti(c):
+        return c * erf(k * c) + exp(-(k * c) ** 2) / (k * sqrt(pi))
+
+    def inner(s):  # x3 and x4 integrals at fixed s = x5 + x6
+        c0 = float(offset) + 0.1 * s
+        return sqrt(pi) / (16 * k) * (anti(c0 + 2) - anti(c0) - anti(2 - c0) + anti(4 - c0))
+
+    kern = 0.0
+    for lo_s, hi_s in ((0.0, 1.0), (1.0, 2.0)):
+        xs, ws = _gauss_legendre(lo_s, hi_s, 48)
+        kern += sum(w * inner(s) * (1.0 - abs(s - 1.0)) for s, w in zip(xs, ws))
+    return spline_int * grid_int * kern
+STATUS_NONFINITE = 1 << 30  # cuhre_oracle.h ORC_STATUS_NONFINITE

@@ -9,6 +9,10 @@ CUDA device, and writes:
   ref_phase1_<name>.npz  INTEGRATE_GPU_PHASE1 per-region outputs (value,
                        error, active flag, split axis) on deterministic
                        dyadic region lists, with the inputs
+  ref_interp2d_lclt.npz  quad::Interp2D (GPUQuadInterp2D.cu:50-106) values of
+                       five LC_LT-shaped FP32 tables at query points
+  ref_lclt.json        GPUcuhre::integrate of the LC_LT integrand
+                       (lc_lt_t.h:18-52) on those tables over 3-D boxes
 
     python tests/golden/make_golden.py --out <dir>
 
@@ -55,6 +59,13 @@ INTEGRATE_CASES = [
      [0.3, 0.5, 0.7, 0.45, 0.6], 1e-7, 1e-12),
 ]
 for s in range(4):
+    a, u = product_peak_params(6, s)
+    INTEGRATE_CASES.append((f"config3_productpeak6_seed{s}", "product_peak", 6, a, u, 1e-5,
+                            1e-12))
+# seeds of the batch generator whose breadth-first results miss the
+# analytic value by more than epsrel (the reference engine's own
+# two-phase result on them is recorded beside)
+for s in (206, 1190):
     a, u = product_peak_params(6, s)
     INTEGRATE_CASES.append((f"config3_productpeak6_seed{s}", "product_peak", 6, a, u, 1e-5,
                             1e-12))
@@ -111,8 +122,12 @@ def run_integrate(case):
         raise RuntimeError(f"{name}: rc={out.returncode}\n{out.stderr[-2000:]}")
     line = [ln for ln in out.stdout.splitlines() if ln.startswith("RESULT ")][-1]
     rec = json.loads(line[len("RESULT "):])
+    # the reference prints the leftover count of its first phase
+    # ("Phase2 regions:%i", GPUquad.h:690)
+    boxes = [int(ln.split(":")[1]) for ln in out.stdout.splitlines()
+             if ln.startswith("Phase2 regions:")]
     rec.update({"name": name, "family_name": fam, "a": [float(x) for x in a],
-                "u": [float(x) for x in u]})
+                "u": [float(x) for x in u], "phase2_boxes": boxes[-1] if boxes else None})
     return rec
 
 
@@ -142,6 +157,87 @@ def run_phase1(case, outdir):
     return m
 
 
+# LC_LT boxes (lt, zt, lc) and tolerances of the table fixtures.
+LCLT_CASES = [
+    ("lclt_box1", [1.0, 0.1, 0.0], [100.0, 0.3, 6.0], 1e-5),
+    ("lclt_box2", [5.0, 0.15, 1.0], [60.0, 0.25, 4.0], 1e-6),
+]
+
+
+def lclt_tables_f32():
+    """The LC_LT-shaped synthetic tables (cubature.tables.lclt_data(0))
+    rounded to FP32: the reference's Interp2D holds FP32 textures, so both
+    engines then interpolate the same numbers."""
+    sys.path.insert(0, str(ROOT / "old-gpuintegration_b200"))
+    from cubature import tables as T
+
+    d = T.lclt_data(0)
+    xs = np.asarray(d["xs"], np.float32)
+    ys = np.asarray(d["ys"], np.float32)
+    z = np.stack([np.asarray(t, np.float32) for t in d["z"]])
+    return xs, ys, z
+
+
+def write_tables(fh, xs, ys, z):
+    np.array([len(xs), len(ys), z.shape[0]], dtype=np.int32).tofile(fh)
+    xs.astype(np.float32).tofile(fh)
+    ys.astype(np.float32).tofile(fh)
+    for q in range(z.shape[0]):
+        np.ascontiguousarray(z[q], dtype=np.float32).tofile(fh)
+
+
+def interp_queries(xs, ys, seed=3):
+    """Query points: every knot pair, uniform points inside the table, and
+    points below its first knots (the reference extrapolates from the first
+    cell there; above the last knot it reads past the table, so no query
+    goes there)."""
+    rng = np.random.default_rng(seed)
+    kx, ky = np.meshgrid(xs.astype(np.float64), ys.astype(np.float64), indexing="ij")
+    qx = [kx.ravel(), rng.uniform(xs[0], xs[-1], 2000), rng.uniform(0.5 * xs[0], xs[0], 100)]
+    qy = [ky.ravel(), rng.uniform(ys[0], ys[-1], 2000), rng.uniform(ys[0], ys[-1], 100)]
+    qx.append(rng.uniform(xs[0], xs[-1], 100))
+    qy.append(rng.uniform(0.5 * ys[0], ys[0], 100))
+    return np.concatenate(qx), np.concatenate(qy)
+
+
+def run_tables(outdir):
+    xs, ys, z = lclt_tables_f32()
+    qx, qy = interp_queries(xs, ys)
+    vals = []
+    recs = []
+    with tempfile.TemporaryDirectory() as td:
+        for q in range(z.shape[0]):
+            fin, fout = Path(td) / "in.bin", Path(td) / "out.bin"
+            with open(fin, "wb") as fh:
+                write_tables(fh, xs, ys, z[q:q + 1])
+                np.array([len(qx)], dtype=np.int64).tofile(fh)
+                qx.tofile(fh)
+                qy.tofile(fh)
+            out = subprocess.run([str(DRIVER), "interp2d", str(fin), str(fout)],
+                                 capture_output=True, text=True, timeout=600)
+            if out.returncode != 0:
+                raise RuntimeError(f"interp2d: rc={out.returncode}\n{out.stderr[-2000:]}")
+            vals.append(np.fromfile(fout, dtype=np.float64))
+        tab = Path(td) / "tables.bin"
+        with open(tab, "wb") as fh:
+            write_tables(fh, xs, ys, z)
+        for name, lo, hi, er in LCLT_CASES:
+            args = [str(DRIVER), "lclt", str(tab), repr(er), repr(1e-12),
+                    *[repr(float(v)) for v in lo], *[repr(float(v)) for v in hi]]
+            out = subprocess.run(args, capture_output=True, text=True, timeout=600)
+            if out.returncode != 0:
+                raise RuntimeError(f"{name}: rc={out.returncode}\n{out.stderr[-2000:]}")
+            line = [ln for ln in out.stdout.splitlines() if ln.startswith("RESULT ")][-1]
+            rec = json.loads(line[len("RESULT "):])
+            rec.update({"name": name, "lo": lo, "hi": hi})
+            recs.append(rec)
+            print("lclt", json.dumps(rec), flush=True)
+    np.savez_compressed(outdir / "ref_interp2d_lclt.npz", xs=xs, ys=ys, z=z, qx=qx, qy=qy,
+                        interp=np.stack(vals))
+    (outdir / "ref_lclt.json").write_text(json.dumps(recs, indent=1) + "\n")
+    return len(qx)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=str(Path(__file__).resolve().parent))
@@ -156,6 +252,9 @@ def main():
         for case in PHASE1_CASES:
             m = run_phase1(case, outdir)
             print("phase1", case[0], m, flush=True)
+    if args.only in ("", "tables"):
+        m = run_tables(outdir)
+        print("tables", m, flush=True)
     if args.only in ("", "integrate"):
         recs = []
         for case in INTEGRATE_CASES:

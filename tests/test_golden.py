@@ -91,6 +91,9 @@ def integrate_cases():
 
 
 def phase2_case(rec):
+    """The reference's run reached its second phase (leftover boxes)."""
+    if rec.get("phase2_boxes") is not None:
+        return rec["phase2_boxes"] > 0
     return "phase2" in rec["name"]
 
 
@@ -140,20 +143,24 @@ def test_reference_phase2_deviation(oracle, rec):
 @pytest.mark.gpu
 @pytest.mark.parametrize("rec", integrate_cases(), ids=lambda r: r["name"])
 def test_cuda_integrate_vs_reference(cub, oracle, ctx, rec):
-    """The CUDA engine against the reference engine's own integrate():
-    first-phase runs agree in status, region count (within 1%: the engines
-    sum the rule in different orders, so near-ties can flip) and value
-    (within 2 epsrel); second-phase runs agree in status and land within
-    their error estimate of the analytic value (where the reference does
-    not, see test_reference_phase2_deviation)."""
+    """The CUDA engine against the reference engine's own integrate().
+    Runs that finish in the first phase give the reference's results
+    exactly: the same region count, evaluation count and status, and the
+    same value to rounding (the engines sum the rule in different orders;
+    on every golden case no region's classification sits close enough to
+    its threshold for that to flip it).  Second-phase runs agree in status
+    and land within their error estimate of the analytic value (where the
+    reference does not, see test_reference_phase2_deviation)."""
     n = rec["ndim"]
     r = ctx.integrate(cub.Integrand(rec["family_name"], n, rec["a"], rec["u"]), rec["epsrel"],
                       rec["epsabs"])
     exact = oracle.exact(oracle.make_integrand(rec["family_name"], n, rec["a"], rec["u"]))
     assert r.status == rec["errorFlag"]
     if not phase2_case(rec):
-        assert abs(r.nregions - rec["nregions"]) <= 0.01 * rec["nregions"]
-        assert abs(r.integral - rec["integral"]) <= 2 * rec["epsrel"] * abs(rec["integral"])
+        assert r.nregions == rec["nregions"]
+        assert r.neval == rec["neval"]
+        assert abs(r.integral - rec["integral"]) <= 1e-12 * abs(rec["integral"])
+        assert abs(r.error - rec["error"]) <= 1e-12 * abs(rec["integral"]) + 1e-6 * rec["error"]
     else:
         assert abs(r.nregions - rec["nregions"]) <= 5e-3 * rec["nregions"]
         assert abs(r.integral - exact) <= max(r.error, rec["epsrel"] * abs(exact))

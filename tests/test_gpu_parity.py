@@ -10,8 +10,12 @@ Tolerances (FP64 throughout):
     fourth differences are within 1e-9 (relative) or whose error ratio is
     within 1e-8 of 1 -- there the last bit of exp/cos decides;
   * scan/compact/bisect: bit-exact;
-  * full integrations: |I_gpu - I_cpu| <= 2 epsrel |I| and both within
-    their error estimates of the analytic value; region counts within 2%.
+  * full integrations: the oracle's region count, evaluation count and
+    status exactly, |I_gpu - I_cpu| <= 1e-12 |I| (rounding of different
+    summation orders), and both within their error estimates of the
+    analytic value.  Integrals that enter the depth-first second phase
+    compare their values within 2 epsrel and their region counts within
+    0.5% (the two sides order their heap pops of equal keys differently).
 """
 import math
 import zlib
@@ -171,13 +175,17 @@ CASES = [
 ]
 
 
-def _compare_full(r_g, r_c, exact, epsrel, label, count_tol=0.02):
+def _compare_full(r_g, r_c, exact, epsrel, label, count_tol=5e-3):
     assert r_g.status == r_c["status"], label
-    assert abs(r_g.integral - r_c["value"]) <= 2 * epsrel * abs(r_c["value"]) + 1e-15, label
+    if r_c.get("phase2_regions", 0) == 0:
+        assert r_g.nregions == r_c["nregions"], (label, r_g.nregions, r_c["nregions"])
+        assert r_g.neval == r_c["neval"], label
+        assert abs(r_g.integral - r_c["value"]) <= 1e-12 * abs(r_c["value"]) + 1e-300, label
+    else:
+        assert abs(r_g.integral - r_c["value"]) <= 2 * epsrel * abs(r_c["value"]) + 1e-15, label
+        assert abs(r_g.nregions - r_c["nregions"]) <= count_tol * r_c["nregions"] + 4, label
     if r_c["status"] == 0:
         assert abs(r_g.integral - exact) <= max(10 * r_g.error, 2 * epsrel * abs(exact)), label
-    assert abs(r_g.nregions - r_c["nregions"]) <= count_tol * r_c["nregions"] + 4, label
-    assert r_g.neval > 0
 
 
 @pytest.mark.parametrize("family,n,a,u,epsrel", CASES)
@@ -274,6 +282,39 @@ def test_batch_matches_oracle(cub, oracle, ctx):
     out = ctx.integrate_batch("product_peak", n, params, eps, 1e-12)
     for r_g, (r_c, ex) in zip(out, refs):
         _compare_full(r_g, r_c, ex, eps, "batch")
+
+
+def test_batch_generator_misses_are_the_algorithms_own(cub, oracle, ctx):
+    """Product peaks of the 4096-integral batch generator (6-D, a_i
+    log-uniform in [1, 50], u_i uniform in [0.1, 0.9], seed = index) whose
+    breadth-first results miss the analytic value by more than epsrel while
+    reporting status 0 (seeds 26, 80, 206, 663, 1190: 1.2e-5 .. 3.3e-4
+    relative).  The oracle's restatement of the reference algorithm gives
+    the same region count and the same value to rounding: the miss is the
+    degree-9 rule's optimistic error estimate on these sharp peaks, not the
+    engine."""
+    import math
+
+    seeds = [26, 80, 206, 663, 1190]
+    n, eps = 6, 1e-5
+    params, cases = [], []
+    for k in seeds:
+        rng = np.random.default_rng(k)
+        a = np.exp(rng.uniform(math.log(1.0), math.log(50.0), n))
+        u = rng.uniform(0.1, 0.9, n)
+        params.append(cub.make_params(n, list(a), list(u)))
+        cases.append((a, u))
+    out = ctx.integrate_batch("product_peak", n, params, eps, 1e-12,
+                              cub.options(policy=cub.POLICY_BREADTH))
+    R = oracle.Rule(n)
+    for r_g, (a, u), k in zip(out, cases, seeds):
+        f_c = oracle.make_integrand("product_peak", n, a, u)
+        r_c = R.integrate_reference(f_c, eps, 1e-12, phase1_cap=1 << 28)
+        ex = oracle.exact(f_c)
+        assert r_g.status == r_c["status"] == 0, k
+        assert r_g.nregions == r_c["nregions"], k
+        assert abs(r_g.integral - r_c["value"]) <= 1e-12 * abs(ex), k
+        assert abs(r_g.integral - ex) > eps * abs(ex), k  # the documented miss
 
 
 def test_breadth_policy_converges(cub, oracle, ctx):
@@ -524,6 +565,34 @@ def test_table7_batch_matches_oracle(cub, oracle, ctx):
         _compare_full(r_g, r_c, r_c["value"], eps, ("table7", o))
 
 
+def test_table7_batch_at_stated_epsrel_vs_closed_form(cub, ctx):
+    """The table workload at its stated epsrel 1e-6 (breadth-first, the
+    reference's classification), four of the 256 benchmark offsets, against
+    the closed-form FP64 values of tests/golden/table7_exact.json
+    (tests/golden/make_table7_exact.py): every integral converges (status 0)
+    and lands within epsrel of the closed form."""
+    import json
+    from pathlib import Path
+
+    from cubature import tables as T
+
+    fx = json.loads((Path(__file__).resolve().parent / "golden" / "table7_exact.json").read_text())
+    pick = [0, 85, 170, 255]
+    offs = [fx["offsets"][i] for i in pick]
+    eps = 1e-6
+    tab = T.Table7(T.table7_data(0), 0)
+    # epsabs small enough that the per-region absolute allowance, summed
+    # over the ~2e7 regions, stays far below epsrel |I| (with 1e-12 the
+    # reference's test lets regions finish on epsabs alone, and the result
+    # lands within its error estimate but ~3e-6 from the value)
+    out = ctx.integrate_table7_batch(tab, offs, eps, 1e-15,
+                                     cub.options(policy=cub.POLICY_BREADTH))
+    for r_g, i in zip(out, pick):
+        exact = fx["exact"][i]
+        assert r_g.status == 0, (i, r_g)
+        assert abs(r_g.integral - exact) <= eps * abs(exact), (i, r_g.integral, exact)
+
+
 def test_autotune_picks_a_working_tiling(cub, ctx):
     """The autotuner returns one of its candidates, and the batch integrated
     with it gives the default options' answers."""
@@ -666,3 +735,60 @@ def test_graph_rejects_oversized_grid(cub, ctx):
     assert e.value.code == cub.ERR_UNSUPPORTED
     with pytest.raises(cub.CubatureError):
         ctx.graph([("gaussian", 1, 4)])
+
+
+REPLICATED_CASES = [
+    ("oscillatory", 8, 1.1, 0.3, 1e-6),
+    ("corner_peak", 8, 0.5, 0.0, 1e-6),
+    ("gaussian", 5, 5.0, 0.5, 1e-3),
+    ("gaussian", 3, [4.0, 6.0, 5.0], [0.3, 0.5, 0.6], 1e-7),
+    ("product_peak", 4, [8.0, 12.0, 6.0, 10.0], [0.3, 0.6, 0.5, 0.4], 1e-5),
+    ("continuous", 2, [3.0, 4.0], [0.4, 0.6], 1e-5),
+    ("cossum", 6, 1.0, 0.0, 1e-4),
+]
+
+
+def _same_bits(a, b, label):
+    assert (a.integral == b.integral and a.error == b.error and a.nregions == b.nregions
+            and a.neval == b.neval and a.status == b.status and a.iterations == b.iterations), \
+        (label, a, b)
+
+
+@pytest.mark.parametrize("family,n,a,u,epsrel", REPLICATED_CASES)
+def test_replicated_kernel_bit_identical(cub, ctx, family, n, a, u, epsrel):
+    """The replicated-decision kernel (batches of at most 32 integrals on
+    short lists) and the persistent kernel compute the same rule sums in the
+    same order and take the same decisions: identical results, bit for
+    bit, including runs whose lists outgrow the replicated kernel's range
+    and continue in the other drivers."""
+    f = cub.Integrand(family, n, a, u)
+    for max_n in (0, 96):
+        o_rep = cub.options(persistent_max_n=max_n)
+        o_old = cub.options(persistent_max_n=max_n, replicated=False)
+        r1 = ctx.integrate(f, epsrel, 1e-12, o_rep)
+        r2 = ctx.integrate(f, epsrel, 1e-12, o_old)
+        _same_bits(r1, r2, (family, n, max_n))
+
+
+def test_replicated_kernel_bit_identical_batches(cub, ctx):
+    """Small batches (one list, several integrals, uneven difficulty), the
+    reference policy with a phase-1 cap that hands boxes to phase 2, and
+    non-unit boxes: the two kernels agree bit for bit."""
+    rng = np.random.default_rng(7)
+    n = 5
+    params = [cub.make_params(n, list(np.exp(rng.uniform(0, np.log(20), n))),
+                              list(rng.uniform(0.2, 0.8, n))) for _ in range(12)]
+    for opts in ({}, {"phase1_cap": 2048}, {"policy": cub.POLICY_BREADTH}):
+        r1 = ctx.integrate_batch("product_peak", n, params, 1e-5, 1e-12, cub.options(**opts))
+        r2 = ctx.integrate_batch("product_peak", n, params, 1e-5, 1e-12,
+                                 cub.options(replicated=False, **opts))
+        for k, (x, y) in enumerate(zip(r1, r2)):
+            _same_bits(x, y, (opts, k))
+    lo = [[-1.0] * 3, [0.0, 0.5, 0.0]]
+    hi = [[1.0] * 3, [2.0, 1.5, 0.5]]
+    gp = [cub.make_params(3, [2.0, 3.0, 1.5], [0.2, 0.9, 0.1])] * 2
+    r1 = ctx.integrate_batch("gaussian", 3, gp, 1e-7, 1e-12, lo=lo, hi=hi)
+    r2 = ctx.integrate_batch("gaussian", 3, gp, 1e-7, 1e-12, cub.options(replicated=False),
+                             lo=lo, hi=hi)
+    for x, y in zip(r1, r2):
+        _same_bits(x, y, "box")

@@ -96,3 +96,64 @@ def test_synthetic_tables_are_seeded_and_positive():
     assert o.shape == (256,) and o.min() >= -1 and o.max() <= 1
     L = T.lclt_data(0)
     assert L["xs"].shape == (22,) and L["ys"].shape == (5,) and len(L["z"]) == 5
+
+
+def _table7_bruteforce(oracle, d, offset, n=40):
+    """The 7-D table integral by tensor Gauss-Legendre: the spline with 4
+    points per knot cell (exact for its cubics), the bilinear grid by its
+    trapezoid sum, the 4-D kernel with n points per axis."""
+    sx, sy = d["spline_x"], d["spline_y"]
+    sp = oracle.spline1d(sx, sy)
+    xg, wg = np.polynomial.legendre.leggauss(4)
+    s_int = 0.0
+    for i in range(len(sx) - 1):
+        a, b = sx[i], sx[i + 1]
+        for x, w in zip(0.5 * (b - a) * xg + 0.5 * (a + b), 0.5 * (b - a) * wg):
+            s_int += w * oracle.spline_eval(sp, x)
+    gx, gy, gz = d["grid_x"], d["grid_y"], d["grid_z"]
+    g_int = np.sum(np.outer(np.diff(gx), np.diff(gy)) / 4 *
+                   (gz[:-1, :-1] + gz[1:, :-1] + gz[:-1, 1:] + gz[1:, 1:]))
+    x, w = np.polynomial.legendre.leggauss(n)
+    x, w = 0.5 * x + 0.5, 0.5 * w
+    X3, X4, X5, X6 = np.meshgrid(x, x, x, x, indexing="ij")
+    W = np.einsum("i,j,k,l->ijkl", w, w, w, w)
+    r = 4 * X3 - (offset + 2 * X4 + 0.1 * (X5 + X6))
+    k_int = np.sum(W * np.exp(-r * r / (2 * d["sigma"] ** 2)))
+    return s_int * g_int * k_int
+
+
+def test_table7_exact_matches_bruteforce(oracle):
+    """The closed form of the 7-D table integral agrees with a tensor
+    Gauss-Legendre evaluation of the same integrand to 1e-13."""
+    from cubature import tables as T
+
+    d = T.table7_data(0)
+    for o in list(T.table7_offsets(256)[:2]) + [-1.0, 1.0]:
+        ex = oracle.table7_exact(d["spline_x"], d["spline_y"], d["grid_x"], d["grid_y"],
+                                 d["grid_z"], d["sigma"], o)
+        bf = _table7_bruteforce(oracle, d, o)
+        assert abs(ex - bf) <= 1e-13 * abs(ex), (o, ex, bf)
+
+
+def test_table7_exact_fixture(oracle):
+    """tests/golden/table7_exact.json (tests/golden/make_table7_exact.py)
+    holds the closed-form values of all 256 benchmark offsets; the oracle
+    reproduces them, and its adaptive integration agrees at epsrel 1e-4."""
+    import json
+    from pathlib import Path
+
+    from cubature import tables as T
+
+    fx = json.loads((Path(__file__).resolve().parent / "golden" / "table7_exact.json").read_text())
+    d = T.table7_data(0)
+    offs = T.table7_offsets(256)
+    assert np.array_equal(np.array(fx["offsets"]), offs)
+    for i in (0, 17, 255):
+        ex = oracle.table7_exact(d["spline_x"], d["spline_y"], d["grid_x"], d["grid_y"],
+                                 d["grid_z"], d["sigma"], offs[i])
+        assert ex == fx["exact"][i]
+    f = oracle.make_table7(d["spline_x"], d["spline_y"], d["grid_x"], d["grid_y"], d["grid_z"],
+                           d["sigma"], offs[0])
+    g = oracle.Rule(7).integrate_global(f, 1e-4, 1e-12)
+    assert g["status"] == 0
+    assert abs(g["value"] - fx["exact"][0]) <= 1e-4 * abs(fx["exact"][0])
