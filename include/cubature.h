@@ -211,6 +211,24 @@ int cub_integrate_mixed_batch(cub_ctx* ctx, int ndim, int count, const int* fami
                               const double* epsabs, double epsrel0, double epsabs0,
                               const cub_options* opt, cub_result* out);
 
+/* One integral with its second phase split over `world` processes (the
+ * reference's multi-device path, GPUquad.h:430-609 and
+ * GPUKernelquad.cu:729-906).  Every caller runs the same first phase (it is
+ * deterministic, so all agree on the leftover boxes without exchanging
+ * them) and refines share `rank` of the leftover boxes: world contiguous
+ * parts of the leftover list, the last taking the remainder
+ * (GPUKernelquad.cu:759-768).  *phase1 receives the first phase's result
+ * (its finished sums, regions and evaluations; the whole result when no box
+ * was left, with *part zeroed); *part the share's value and error sums,
+ * regions, evaluations, and its failed boxes in `status` (or
+ * CUB_STATUS_NONFINITE).  The combined result is phase1 plus the sum of all
+ * parts, with status = the summed failed boxes unless
+ * error <= max(epsrel |value|, epsabs) (GPUquad.h:713); the Python binding
+ * does that with one all-reduce (cubature.parallel.integrate_split). */
+int cub_integrate_shard(cub_ctx* ctx, int family, int ndim, const cub_genz_params* params,
+                        double epsrel, double epsabs, const cub_options* opt, int rank,
+                        int world, cub_result* phase1, cub_result* part);
+
 /* cub_integrate over the box [lo, hi] (ndim values each, host memory,
  * finite, hi > lo) instead of the unit cube: the reference's Volume
  * argument (GPUQuadVolume.cu:4-25, GPUQuadSample.cu:44-56,174-179), here in

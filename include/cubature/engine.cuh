@@ -49,6 +49,12 @@ struct Options {
   int replicated = 1;             // small batches: the replicated-decision kernel for short lists
   long long barrier_spins = 0;    // grid-barrier polls before a timeout; 0 = kBarrierSpins
   int hold_block = -1;            // tests: this block never arrives at a grid barrier
+  // Second phase on share shard_rank of shard_world of the leftover boxes
+  // (the reference's multi-device cut, GPUKernelquad.cu:759-768).  The
+  // results then hold only the share's depth-first sums, regions and
+  // failed boxes; Workspace::phase1_out receives the first phase's.
+  int shard_rank = 0;
+  int shard_world = 1;
 };
 
 struct Result {
@@ -207,6 +213,11 @@ class Workspace {
   int* heap = nullptr;
   int* counter = nullptr;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  // When set, run_batch stores each integral's first-phase result here
+  // before its second phase (integrals without leftover boxes: the final
+  // result).
+  Result* phase1_out = nullptr;
+  int counter_host = 0;  // host source of the phase-2 box counter's start
 
   long long cap() const { return cap_; }
   long long left_cap() const { return left_cap_; }
@@ -950,26 +961,69 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
     n_left = nx.n_left;
   }
 
+  const bool shard = opt.shard_world > 1;
+  if (status == kOk && n_left > 0 && (ws.phase1_out || shard)) {
+    // the first phase's results, before the second phase adds to them
+    if (!states_fresh) {
+      if (!ws.ck(cudaMemcpyAsync(h, ws.ist, sizeof(IntegralState) * nint,
+                                 cudaMemcpyDeviceToHost, s)) ||
+          !ws.ck(cudaStreamSynchronize(s)))
+        return kErrCuda;
+      st.d2h_bytes += (long long)(sizeof(IntegralState) * nint);
+      states_fresh = true;
+    }
+    if (ws.phase1_out) detail::state_results(h, nint, ws.phase1_out);
+    if (shard) {
+      // the share's sums start from zero
+      for (int k = 0; k < nint; ++k)
+        if (h[k].state == kStatePhase2) {
+          h[k].value = h[k].error = 0;
+          h[k].nregions = h[k].neval = 0;
+        }
+      if (!ws.ck(cudaMemcpyAsync(ws.ist, h, sizeof(IntegralState) * nint,
+                                 cudaMemcpyHostToDevice, s)))
+        return kErrCuda;
+      st.h2d_bytes += (long long)(sizeof(IntegralState) * nint);
+    }
+  } else if (ws.phase1_out && status == kOk) {
+    ws.phase1_out = nullptr;  // filled from the final results below
+  }
+  long long box0 = 0, box1 = n_left;
+  if (shard && n_left > 0) {
+    const long long each = n_left / opt.shard_world;
+    box0 = (long long)opt.shard_rank * each;
+    box1 = opt.shard_rank == opt.shard_world - 1 ? n_left : box0 + each;
+  }
   if (status == kOk && n_left > 0) {
-    // phase 2 on the leftover boxes
+    // phase 2 on the leftover boxes [box0, box1)
     states_fresh = false;
     int dev_blocks = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&dev_blocks, k_phase2<N, Src>, 128, 0);
     dev_blocks = std::max(1, dev_blocks);
-    long long blocks = std::min<long long>((long long)sms * dev_blocks, (n_left + 3) / 4);
+    long long blocks = std::min<long long>((long long)sms * dev_blocks, (box1 - box0 + 3) / 4);
     blocks = std::max<long long>(blocks, 1);
     const long long nwarps = blocks * 4;
     const int stride = opt.phase2_max_regions + 2;
     if (!ws.reserve_slab(sizeof(P2Region<N>) * nwarps * stride,
                          (size_t)nwarps * stride * (sizeof(P2HeapEnt) / sizeof(int))))
       return kErrCuda;
-    if (!ws.ck(cudaMemsetAsync(ws.counter, 0, sizeof(int), s))) return kErrCuda;
+    if (shard) {
+      // boxes of other shares contribute nothing to the collection
+      if (!ws.ck(cudaMemsetAsync(ws.left_res, 0, sizeof(LeftoverResult) * n_left, s)))
+        return kErrCuda;
+      ws.counter_host = (int)box0;
+      if (!ws.ck(cudaMemcpyAsync(ws.counter, &ws.counter_host, sizeof(int),
+                                 cudaMemcpyHostToDevice, s)))
+        return kErrCuda;
+    } else if (!ws.ck(cudaMemsetAsync(ws.counter, 0, sizeof(int), s))) {
+      return kErrCuda;
+    }
     Phase2Args p;
     p.left_lo = ws.left_lo;
     p.left_len = ws.left_len;
     p.left_rid = ws.left_rid;
     p.left_cap = ws.left_cap();
-    p.n_left = (int)n_left;
+    p.n_left = (int)box1;
     p.max_regions = opt.phase2_max_regions;
     p.slab = ws.slab;
     p.heap = reinterpret_cast<P2HeapEnt*>(ws.heap);
@@ -979,9 +1033,9 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
     if (ws.timing) ws.ck(cudaEventRecord(ws.ev[2], s));
     k_phase2<N, Src><<<(unsigned)blocks, 128, 0, s>>>(src, T, p);
     if (ws.timing) ws.ck(cudaEventRecord(ws.ev[3], s));
-    st.phase2_boxes += n_left;
+    st.phase2_boxes += box1 - box0;
     const unsigned cb = (unsigned)std::max(1, std::min((nint + 7) / 8, sms * 16));
-    k_phase2_collect<<<cb, 256, 0, s>>>(ws.ist, nint, ws.left_res, T.npoints);
+    k_phase2_collect<<<cb, 256, 0, s>>>(ws.ist, nint, ws.left_res, T.npoints, shard ? 0 : 1);
     st.launches += 2;
   }
 

@@ -261,21 +261,25 @@ __global__ void __launch_bounds__(128, 3) k_phase2(Src src, RuleTables T, Phase2
 
 // Per-integral sums of the phase-2 results, one warp per integral, and the
 // final status (GPUKernelquad.cu:870-892, GPUquad.h:713-714).
+// final_test: apply the reference's status test (GPUquad.h:713) to the
+// integral's total; 0 for a share of the boxes (the combined total is
+// tested by the caller), whose status is then its failed-box count.
 static __global__ void k_phase2_collect(IntegralState* ist, int nint, const LeftoverResult* res,
-                                 int npoints) {
+                                        int npoints, int final_test) {
   const int lane = threadIdx.x & 31;
   for (int k = (blockIdx.x * blockDim.x + threadIdx.x) / 32; k < nint;
        k += gridDim.x * blockDim.x / 32) {
     IntegralState& is = ist[k];
     if (is.state != kStatePhase2) continue;
     double v = 0, e = 0;
-    unsigned long long nr = 0;
+    unsigned long long nr = 0, nb = 0;
     int nf = 0;
     for (int j = lane; j < is.left_count; j += 32) {
       const LeftoverResult r = res[is.left_start + j];
       v += r.value;
       e += r.error;
       nr += (unsigned long long)r.nregions;
+      nb += r.nregions > 0 ? 1ull : 0ull;  // boxes refined here (all, unless sharded)
       nf += r.failed;
     }
 #pragma unroll
@@ -283,16 +287,17 @@ static __global__ void k_phase2_collect(IntegralState* ist, int nint, const Left
       v += __shfl_xor_sync(0xffffffffu, v, off);
       e += __shfl_xor_sync(0xffffffffu, e, off);
       nr += __shfl_xor_sync(0xffffffffu, nr, off);
+      nb += __shfl_xor_sync(0xffffffffu, nb, off);
       nf += __shfl_xor_sync(0xffffffffu, nf, off);
     }
     if (lane == 0) {
-      const unsigned long long n = (unsigned long long)is.left_count;
+      const unsigned long long n = nb;
       is.value += v;
       is.error += e;
       is.nregions += nr;
       is.neval += (nr - n) * (unsigned long long)npoints * 2ull + n * (unsigned long long)npoints;
       is.status = nf;
-      if (is.error <= detail::max_err(is.value, is.epsrel, is.epsabs)) is.status = 0;
+      if (final_test && is.error <= detail::max_err(is.value, is.epsrel, is.epsabs)) is.status = 0;
       if (!isfinite(v) || !isfinite(e)) is.status = kStatusNonFinite;
       is.state = kStateDone;
     }

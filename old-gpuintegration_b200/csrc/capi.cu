@@ -296,6 +296,8 @@ int integrate_impl(cub_ctx* ctx, int family, int ndim, int count, const cub_genz
   }
   Options o = to_options(opt);
   if (o.max_slots <= 0) o.max_slots = ctx->ws->auto_slots(ndim, o.policy);
+  o.shard_rank = ctx->shard_rank;
+  o.shard_world = ctx->shard_world;
   std::vector<Result> res;
   std::vector<GenzParams> hp;
   std::vector<double> ger, gea, gbox;
@@ -365,6 +367,39 @@ int cub_integrate(cub_ctx* ctx, int family, int ndim, const cub_genz_params* par
                   double epsrel, double epsabs, const cub_options* opt, cub_result* out) {
   return integrate_impl(ctx, family, ndim, 1, params, nullptr, nullptr, nullptr, nullptr, epsrel,
                         epsabs, opt, out);
+}
+
+int cub_integrate_shard(cub_ctx* ctx, int family, int ndim, const cub_genz_params* params,
+                        double epsrel, double epsabs, const cub_options* opt, int rank,
+                        int world, cub_result* phase1, cub_result* part) {
+  if (!ctx || !phase1 || !part || world < 1 || rank < 0 || rank >= world) {
+    set_error("invalid argument: need 0 <= rank < world and both outputs");
+    return CUB_ERR_INVALID;
+  }
+  cub_options o;
+  if (opt)
+    o = *opt;
+  else
+    cub_default_options(&o);
+  Result p1{};
+  ctx->ws->phase1_out = &p1;
+  ctx->shard_rank = rank;
+  ctx->shard_world = world;
+  const int rc = integrate_impl(ctx, family, ndim, 1, params, nullptr, nullptr, nullptr, nullptr,
+                                epsrel, epsabs, &o, part);
+  const bool split = ctx->ws->phase1_out != nullptr;
+  ctx->ws->phase1_out = nullptr;
+  ctx->shard_rank = 0;
+  ctx->shard_world = 1;
+  if (rc < 0) return rc;
+  if (split) {
+    result_to_c(p1, phase1);
+  } else {
+    // finished in the first phase: every rank holds the whole result
+    *phase1 = *part;
+    std::memset(part, 0, sizeof(*part));
+  }
+  return 0;
 }
 
 int cub_integrate_box(cub_ctx* ctx, int family, int ndim, const cub_genz_params* params,

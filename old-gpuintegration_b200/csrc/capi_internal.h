@@ -12,6 +12,10 @@
 
 struct cub_ctx {
   int device = 0;
+  // share of the second phase the next integrate call refines
+  // (cub_integrate_shard); 0 of 1 otherwise
+  int shard_rank = 0;
+  int shard_world = 1;
   cudaStream_t stream = nullptr;
   cubature::Workspace* ws = nullptr;
   cubature::GenzParams* d_params = nullptr;

@@ -134,7 +134,7 @@ EXPORTS = (
     "cub_mlp_set_data", "cub_mlp_params", "cub_mlp_grad", "cub_mlp_train", "cub_mlp_eval",
     "cub_cv_default_options", "cub_cv_integrate_batch", "cub_autotune_batch",
     "cub_integrate_mixed_batch", "cub_graph_create", "cub_graph_launch", "cub_graph_info",
-    "cub_graph_destroy", "cub_fp64_peak",
+    "cub_graph_destroy", "cub_fp64_peak", "cub_integrate_shard",
 )
 
 _lib = None
@@ -220,6 +220,9 @@ def load_library(path: str | Path | None = None):
     L.cub_split_noalloc.argtypes = [C.c_int, C.c_longlong, vp, vp, C.c_longlong, vp, vp, vp, vp,
                                     C.c_longlong, C.c_int, vp, vp]
     L.cub_fp64_peak.argtypes = [C.c_int, dp]
+    L.cub_integrate_shard.argtypes = [vp, C.c_int, C.c_int, C.POINTER(GenzParams), C.c_double,
+                                      C.c_double, C.POINTER(COptions), C.c_int, C.c_int,
+                                      C.POINTER(CResult), C.POINTER(CResult)]
     if path is None:
         _lib = L
     return L
@@ -407,6 +410,19 @@ class Context:
             _check(self._lib.cub_integrate_box(self._h, family_id(f.family), f.ndim, C.byref(p),
                                                blo, bhi, epsrel, epsabs, o, C.byref(out)))
         return Result.from_c(out)
+
+    def integrate_shard(self, f: Integrand, epsrel: float, epsabs: float, rank: int, world: int,
+                        opts: COptions | None = None) -> tuple[Result, Result]:
+        """The first phase of f and share `rank` of `world` of its second
+        phase (cub_integrate_shard): (first-phase result, the share's
+        part).  cubature.parallel.integrate_split combines the parts."""
+        p1, part = CResult(), CResult()
+        p = f.params()
+        o = C.byref(opts) if opts else None
+        _check(self._lib.cub_integrate_shard(self._h, family_id(f.family), f.ndim, C.byref(p),
+                                             epsrel, epsabs, o, rank, world, C.byref(p1),
+                                             C.byref(part)))
+        return Result.from_c(p1), Result.from_c(part)
 
     def integrate_batch(self, family, ndim: int, params: Sequence[GenzParams], epsrel,
                         epsabs, opts: COptions | None = None, lo=None, hi=None) -> list[Result]:

@@ -1,12 +1,19 @@
-"""Independent integrals sharded across GPUs, one process per GPU.
+"""Work split across GPUs, one process per GPU (torch.distributed: NCCL
+between GPUs, gloo on CPU).
 
-The reference distributes one integral's leftover regions over devices with
-MPI or OpenMP (GPUquad.h:430-609, GPUKernelquad.cu:729-906).  Here the unit
-of work is a whole integral: a batch of independent integrals is cut into
-contiguous shards, one per rank (torch.distributed, NCCL between GPUs or
-gloo on CPU), and each rank integrates its shard on its own device with no
-communication on the data path.  One gather of fixed-size result records at
-the end gives every rank the full result list.
+* Batches of independent integrals (integrate_sharded): the batch is cut
+  into contiguous shards, one per rank, and each rank integrates its shard
+  on its own device with no communication on the data path.  One gather of
+  fixed-size result records at the end gives every rank the full list.
+* One integral (integrate_split): the reference's own multi-device split
+  (GPUquad.h:430-609, GPUKernelquad.cu:729-906).  Every rank runs the same
+  breadth-first first phase (deterministic, so the ranks agree on the
+  leftover boxes without exchanging them), refines a contiguous share of
+  the leftover boxes depth-first (the reference's cut,
+  GPUKernelquad.cu:759-768), and one all-reduce of a few FP64 numbers --
+  value, error, regions, evaluations, failed boxes, non-finite flag --
+  combines the shares.  The reference's final status test follows
+  (GPUquad.h:713).
 
 Failures are collective: a rank whose shard raises still joins the gather
 with an error mark, and every rank then raises, so no rank waits on a peer
@@ -85,6 +92,64 @@ def integrate_sharded(integrate: Callable[[int, int], Sequence[Result]], count: 
         host = parts[r].cpu()
         out.extend(_unpack(host[i]) for i in range(b - a))
     return out
+
+
+_NONFINITE = 1 << 30
+
+
+def integrate_split(shard: Callable[[int, int], tuple], epsrel: float, epsabs: float,
+                    group=None) -> Result:
+    """One integral with its second phase split over the ranks.
+
+    shard(rank, world) runs the first phase and this rank's share of the
+    leftover boxes and returns (phase1, part): the first phase's result
+    (finished sums, or the converged result when no box was left) and the
+    share's value, error, regions and evaluations with its failed-box count
+    in `status` (or the non-finite status).  Every rank returns the same
+    combined Result.  Without a process group this is the world-1 case."""
+    if dist.is_available() and dist.is_initialized():
+        world, rank = dist.get_world_size(group), dist.get_rank(group)
+    else:
+        world, rank, group = 1, 0, None
+    failed, message = 0.0, ""
+    p1 = part = None
+    try:
+        p1, part = shard(rank, world)
+    except Exception as exc:  # every rank must still reach the all-reduce
+        failed, message = 1.0, f"rank {rank}: {exc}"
+    if part is not None:
+        nonfin = 1.0 if part.status == _NONFINITE else 0.0
+        fail_boxes = 0.0 if part.status == _NONFINITE else float(part.status)
+        vec = [part.integral, part.error, float(part.nregions), float(part.neval), fail_boxes,
+               nonfin, failed]
+    else:
+        vec = [0.0] * 6 + [failed]
+    if world > 1:
+        device = torch.device("cuda", torch.cuda.current_device()) \
+            if dist.get_backend(group) == "nccl" else torch.device("cpu")
+        t = torch.tensor(vec, dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+        vec = [float(x) for x in t.cpu()]
+    if vec[6] != 0.0:
+        raise CubatureError(ERR_INVALID, message or "integration failed on another rank")
+    value = p1.integral + vec[0]
+    error = p1.error + vec[1]
+    nonfinite = vec[5] != 0.0 or p1.status == _NONFINITE
+    status = int(vec[4])
+    if error <= max(epsrel * abs(value), epsabs):
+        status = 0
+    if nonfinite:
+        status = _NONFINITE
+    return Result(integral=value, error=error, nregions=p1.nregions + int(vec[2]),
+                  neval=p1.neval + int(vec[3]), status=status, iterations=p1.iterations,
+                  state=1)
+
+
+def integrate_split_engine(ctx, f, epsrel: float, epsabs: float, opts=None,
+                           group=None) -> Result:
+    """integrate_split with this rank's GPU engine (ctx.integrate_shard)."""
+    return integrate_split(lambda r, w: ctx.integrate_shard(f, epsrel, epsabs, r, w, opts),
+                           epsrel, epsabs, group)
 
 
 def integrate_batch_sharded(ctx, family, ndim: int, params: Sequence, epsrel, epsabs,

@@ -784,11 +784,22 @@ int orc_phase2_box(const orc_rule* r, const orc_integrand* f, const double* L,
  * Two-phase integration with the reference policy (GPUquad.h:611-727,
  * GPUKernelquad.cu:509-668 and :672-911).
  * ---------------------------------------------------------------------- */
-int orc_integrate_reference(const orc_rule* r, const orc_integrand* f, double epsrel,
-                            double epsabs, int phase1_cap, int phase2_max, int nthreads,
-                            orc_out* out)
+/* The two phases with the second one restricted to a contiguous share of
+ * the leftover boxes: share `rank` of `world`, cut as the reference cuts
+ * its leftover list across devices (GPUKernelquad.cu:759-768: world equal
+ * parts, the last one taking the remainder).  p1 receives the first
+ * phase's result (its finished sums, or the converged result when no box
+ * is left; phase2_regions = leftover boxes), part the share's boxes (their
+ * value and error sums, regions, evaluations; status = failed boxes, or
+ * ORC_STATUS_NONFINITE).  Every rank computes the same first phase. */
+int orc_integrate_reference_shard(const orc_rule* r, const orc_integrand* f, double epsrel,
+                                  double epsabs, int phase1_cap, int phase2_max, int nthreads,
+                                  int rank, int world, orc_out* p1, orc_out* part)
 {
   if (phase2_max <= 0) phase2_max = 2048; /* MAX_GLOBALPOOL_SIZE, quad.h:9 */
+  if (world < 1 || rank < 0 || rank >= world) return -1;
+  orc_out scratch;
+  orc_out* out = &scratch;
   const int nd = r->ndim;
   const size_t fe = (size_t)r->npts;
   if (phase1_cap <= 0) phase1_cap = 1 << 14; /* FIRST_PHASE_MAXREGIONS, quad.h:21 */
@@ -847,10 +858,25 @@ int orc_integrate_reference(const orc_rule* r, const orc_integrand* f, double ep
     if (n < 1) break;
     if (n >= (size_t)phase1_cap) break;
   }
+  memset(p1, 0, sizeof(*p1));
+  memset(part, 0, sizeof(*part));
+  p1->value = integral;
+  p1->error = error;
+  p1->nregions = nregions;
+  p1->neval = neval;
+  p1->phase1_iters = iters;
+  p1->phase2_regions = n;
+  p1->status = nonfinite ? ORC_STATUS_NONFINITE : 0;
   out->phase1_iters = iters;
   out->phase2_regions = n;
 
   int status = 0;
+  size_t first = 0, last = n;
+  if (world > 1) {
+    const size_t each = n / (size_t)world;
+    first = (size_t)rank * each;
+    last = rank == world - 1 ? n : first + each;
+  }
   if (n > 0) {
     double* res = (double*)malloc(sizeof(double) * n);
     double* er = (double*)malloc(sizeof(double) * n);
@@ -861,6 +887,13 @@ int orc_integrate_reference(const orc_rule* r, const orc_integrand* f, double ep
 #pragma omp parallel for schedule(dynamic, 1) num_threads(nt)
 #endif
     for (long long i = 0; i < (long long)n; ++i) {
+      if ((size_t)i < first || (size_t)i >= last) {
+        res[i] = 0;
+        er[i] = 0;
+        cnt[i] = 0;
+        fail[i] = 0;
+        continue;
+      }
       double L[ORC_MAXDIM], W[ORC_MAXDIM];
       for (int d = 0; d < nd; ++d) {
         L[d] = lo[(size_t)d * n + i];
@@ -869,15 +902,25 @@ int orc_integrate_reference(const orc_rule* r, const orc_integrand* f, double ep
       cnt[i] = orc_phase2_box(r, f, L, W, epsrel, epsabs, phase2_max, &res[i], &er[i], &fail[i]);
     }
     size_t total = 0, failed = 0;
+    int part_nonfinite = 0;
     for (size_t i = 0; i < n; ++i) {
       total += (size_t)cnt[i];
       failed += (size_t)fail[i];
-      if (!isfinite(res[i]) || !isfinite(er[i])) nonfinite = 1;
+      if (!isfinite(res[i]) || !isfinite(er[i])) part_nonfinite = 1;
     }
-    integral += psum(res, n);
-    error += psum(er, n);
+    const size_t nb = last - first;
+    part->value = psum(res, n);
+    part->error = psum(er, n);
+    part->nregions = total;
+    part->neval = (total - nb) * fe * 2 + nb * fe;
+    part->phase2_regions = nb;
+    part->phase2_failed = failed;
+    part->status = part_nonfinite ? ORC_STATUS_NONFINITE : (int)failed;
+    nonfinite |= part_nonfinite;
+    integral += part->value;
+    error += part->error;
     nregions += total;
-    neval += (total - n) * fe * 2 + n * fe;
+    neval += part->neval;
     status = (int)failed;
     out->phase2_failed = failed;
     free(res); free(er); free(cnt); free(fail);
@@ -886,12 +929,43 @@ int orc_integrate_reference(const orc_rule* r, const orc_integrand* f, double ep
   if (nonfinite) status = ORC_STATUS_NONFINITE;
   free(lo);
   free(len);
-  out->value = integral;
-  out->error = error;
-  out->nregions = nregions;
-  out->neval = neval;
-  out->status = status;
-  return status;
+  (void)status;
+  return 0;
+}
+
+/* The shares of all ranks combined: value, error, regions, evaluations
+ * and failed boxes summed, and the reference's final status test
+ * (GPUquad.h:713). */
+void orc_combine_shards(const orc_out* p1, const orc_out* parts, int world, double epsrel,
+                        double epsabs, orc_out* out)
+{
+  *out = *p1;
+  size_t failed = 0;
+  int nonfinite = p1->status == ORC_STATUS_NONFINITE;
+  for (int k = 0; k < world; ++k) {
+    out->value += parts[k].value;
+    out->error += parts[k].error;
+    out->nregions += parts[k].nregions;
+    out->neval += parts[k].neval;
+    failed += parts[k].phase2_failed;
+    nonfinite |= parts[k].status == ORC_STATUS_NONFINITE;
+  }
+  out->phase2_failed = failed;
+  int status = (int)failed;
+  if (out->error <= max_err(out->value, epsrel, epsabs)) status = 0;
+  out->status = nonfinite ? ORC_STATUS_NONFINITE : status;
+}
+
+int orc_integrate_reference(const orc_rule* r, const orc_integrand* f, double epsrel,
+                            double epsabs, int phase1_cap, int phase2_max, int nthreads,
+                            orc_out* out)
+{
+  orc_out p1, part;
+  if (orc_integrate_reference_shard(r, f, epsrel, epsabs, phase1_cap, phase2_max, nthreads, 0,
+                                    1, &p1, &part))
+    return -1;
+  orc_combine_shards(&p1, &part, 1, epsrel, epsabs, out);
+  return out->status;
 }
 
 /* ------------------------------------------------------------------------

@@ -182,6 +182,13 @@ int orc_phase2_box(const orc_rule* r, const orc_integrand* f, const double* L,
                    int* failed);
 
 /* ---- full two-phase integration (GPUquad.h:611-727) ---- */
+/* The second phase restricted to share `rank` of `world` of the leftover
+ * boxes (GPUKernelquad.cu:759-768); see cuhre_oracle.c. */
+int orc_integrate_reference_shard(const orc_rule* r, const orc_integrand* f, double epsrel,
+                                  double epsabs, int phase1_cap, int phase2_max, int nthreads,
+                                  int rank, int world, orc_out* p1, orc_out* part);
+void orc_combine_shards(const orc_out* p1, const orc_out* parts, int world, double epsrel,
+                        double epsabs, orc_out* out);
 int orc_integrate_reference(const orc_rule* r, const orc_integrand* f,
                             double epsrel, double epsabs, int phase1_cap,
                             int phase2_max, int nthreads, orc_out* out);

@@ -124,6 +124,13 @@ def lib():
         L.orc_integrate_reference.argtypes = [C.c_void_p, C.POINTER(Integrand), C.c_double,
                                               C.c_double, C.c_int, C.c_int, C.c_int,
                                               C.POINTER(Out)]
+        L.orc_integrate_reference_shard.argtypes = [C.c_void_p, C.POINTER(Integrand),
+                                                    C.c_double, C.c_double, C.c_int, C.c_int,
+                                                    C.c_int, C.c_int, C.c_int, C.POINTER(Out),
+                                                    C.POINTER(Out)]
+        L.orc_combine_shards.argtypes = [C.POINTER(Out), C.POINTER(Out), C.c_int, C.c_double,
+                                         C.c_double, C.POINTER(Out)]
+        L.orc_combine_shards.restype = None
         L.orc_integrate_global.argtypes = [C.c_void_p, C.POINTER(Integrand), C.c_double,
                                            C.c_double, C.c_size_t, C.c_int, C.c_int,
                                            C.POINTER(Out)]
@@ -237,6 +244,18 @@ class Rule:
         lib().orc_integrate_reference(self._h, C.byref(f), epsrel, epsabs, phase1_cap, phase2_max,
                                       nthreads, C.byref(out))
         return out.as_dict()
+
+    def integrate_reference_shard(self, f: Integrand, epsrel, epsabs, rank, world,
+                                  phase1_cap=0, phase2_max=0, nthreads=0):
+        """The two phases with the second one on share `rank` of `world` of
+        the leftover boxes: (first-phase result, the share's part)."""
+        p1, part = Out(), Out()
+        rc = lib().orc_integrate_reference_shard(self._h, C.byref(f), epsrel, epsabs, phase1_cap,
+                                                 phase2_max, nthreads, rank, world, C.byref(p1),
+                                                 C.byref(part))
+        if rc:
+            raise ValueError("bad shard")
+        return p1.as_dict(), part.as_dict()
 
     def integrate_global(self, f: Integrand, epsrel, epsabs, max_regions=1 << 26, max_iters=200,
                          nthreads=0):

@@ -117,7 +117,8 @@ def test_oracle_matches_reference_integrate(oracle, rec):
     assert abs(r["error"] - rec["error"]) <= 1e-13 * abs(rec["integral"]) + 1e-6 * rec["error"]
 
 
-@pytest.mark.parametrize("rec", [r for r in integrate_cases() if phase2_case(r)],
+@pytest.mark.parametrize("rec", [r for r in integrate_cases()
+                                 if phase2_case(r) and not r.get("estimate_miss")],
                          ids=lambda r: r["name"])
 def test_reference_phase2_deviation(oracle, rec):
     """Runs that reach the second phase.  The reference keeps up to 128
@@ -138,6 +139,47 @@ def test_reference_phase2_deviation(oracle, rec):
     theirs = abs(rec["integral"] - exact)
     assert ours <= max(r["error"], rec["epsrel"] * abs(exact))
     assert theirs > 10 * rec["error"]  # the documented deviation
+
+
+@pytest.mark.parametrize("rec", [r for r in integrate_cases() if r.get("rerun")],
+                         ids=lambda r: r["name"])
+def test_reference_phase2_does_not_repeat(oracle, rec):
+    """A second run of tests/golden/make_golden.py on the same B200 gave the
+    reference's second phase different values, region counts and, on the
+    failing case, a different failed-box count (58, then 61): its
+    shared-memory pool spills to device-malloc'ed memory and pulls back an
+    approximate top 64 from work that blocks share, so its result depends on
+    timing.  The oracle (exact heap) returns the same result every time."""
+    rr = rec["rerun"]
+    assert (rr["integral"], rr["nregions"]) != (rec["integral"], rec["nregions"])
+    n = rec["ndim"]
+    f = oracle.make_integrand(rec["family_name"], n, rec["a"], rec["u"])
+    R = oracle.Rule(n)
+    a, b = R.integrate_reference(f, rec["epsrel"], rec["epsabs"]), \
+        R.integrate_reference(f, rec["epsrel"], rec["epsabs"])
+    assert a == b
+
+
+@pytest.mark.parametrize("rec", [r for r in integrate_cases() if r.get("estimate_miss")],
+                         ids=lambda r: r["name"])
+def test_reference_engine_misses_like_the_oracle(oracle, rec):
+    """Seeds of the 4096-integral product-peak generator (6-D, epsrel 1e-5)
+    whose results miss the analytic value by more than epsrel with status
+    0.  The reference engine misses them too (3.3e-4 and 3.8e-4 relative,
+    errorFlag 0): the degree-9 rule's error estimate is optimistic on these
+    sharp peaks.  On seed 206 the oracle's two-phase result equals the
+    reference's to the last digit, with the same region count; on seed 1190
+    the reference's approximate second phase lands further off."""
+    n = rec["ndim"]
+    f = oracle.make_integrand(rec["family_name"], n, rec["a"], rec["u"])
+    r = oracle.Rule(n).integrate_reference(f, rec["epsrel"], rec["epsabs"])
+    exact = oracle.exact(f)
+    assert rec["errorFlag"] == 0 and r["status"] == 0
+    assert abs(rec["integral"] - exact) > rec["epsrel"] * abs(exact)
+    assert abs(r["value"] - exact) > rec["epsrel"] * abs(exact)
+    assert abs(r["nregions"] - rec["nregions"]) <= 1e-3 * rec["nregions"]
+    if rec["name"].endswith("seed206"):
+        assert r["value"] == rec["integral"] and r["nregions"] == rec["nregions"]
 
 
 @pytest.mark.gpu
@@ -161,6 +203,14 @@ def test_cuda_integrate_vs_reference(cub, oracle, ctx, rec):
         assert r.neval == rec["neval"]
         assert abs(r.integral - rec["integral"]) <= 1e-12 * abs(rec["integral"])
         assert abs(r.error - rec["error"]) <= 1e-12 * abs(rec["integral"]) + 1e-6 * rec["error"]
+    elif rec.get("estimate_miss"):
+        # the rule's own miss (test_reference_engine_misses_like_the_oracle):
+        # the engine lands where the oracle's two-phase run does
+        o = oracle.Rule(n).integrate_reference(
+            oracle.make_integrand(rec["family_name"], n, rec["a"], rec["u"]), rec["epsrel"],
+            rec["epsabs"])
+        assert abs(r.nregions - o["nregions"]) <= 5e-3 * o["nregions"]
+        assert abs(r.integral - o["value"]) <= 2 * rec["epsrel"] * abs(o["value"])
     else:
         assert abs(r.nregions - rec["nregions"]) <= 5e-3 * rec["nregions"]
         assert abs(r.integral - exact) <= max(r.error, rec["epsrel"] * abs(exact))

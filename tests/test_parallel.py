@@ -59,12 +59,49 @@ def _oracle_shard(cases, a, b):
     return out
 
 
-def _worker(rank, world, port, count, fail_rank, q):
+# One integral whose first phase leaves boxes for the second (a 512-child
+# cap), for the split of its second phase across ranks.
+SPLIT_CASE = ("product_peak", 4, [30.0, 40.0, 20.0, 35.0], [0.3, 0.6, 0.5, 0.4], 1e-7, 512)
+
+
+def _oracle_split_shard(rank, world):
+    import oracle as O
+
+    fam, n, a, u, eps, cap = SPLIT_CASE
+    p1, part = O.Rule(n).integrate_reference_shard(O.make_integrand(fam, n, a, u), eps, 1e-12,
+                                                   rank, world, phase1_cap=cap)
+    as_res = lambda d: P.Result(d["value"], d["error"], d["nregions"], d["neval"], d["status"],
+                                d["phase1_iters"], 1)
+    return as_res(p1), as_res(part)
+
+
+def _split_worker(rank, world, fail_rank, q):
+    fam, n, a, u, eps, cap = SPLIT_CASE
+
+    def shard(r, w):
+        if r == fail_rank:
+            raise RuntimeError("injected failure")
+        return _oracle_split_shard(r, w)
+
+    try:
+        res = P.integrate_split(shard, eps, 1e-12)
+        q.put((rank, "ok", (res.integral, res.error, res.nregions, res.neval, res.status)))
+    except P.CubatureError as exc:
+        q.put((rank, "error", str(exc)))
+
+
+def _worker(rank, world, port, count, fail_rank, q, mode="batch"):
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     from datetime import timedelta
 
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+    if mode == "split":
+        try:
+            _split_worker(rank, world, fail_rank, q)
+        finally:
+            dist.destroy_process_group()
+        return
     try:
         cases = _cases(count)
 
@@ -88,11 +125,11 @@ def _free_port():
         return s.getsockname()[1]
 
 
-def _run(world, count, fail_rank=-1):
+def _run(world, count, fail_rank=-1, mode="batch"):
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_worker, args=(r, world, port, count, fail_rank, q))
+    procs = [ctx.Process(target=_worker, args=(r, world, port, count, fail_rank, q, mode))
              for r in range(world)]
     for p in procs:
         p.start()
@@ -120,3 +157,43 @@ def test_failure_on_one_rank_reaches_all():
     out = _run(2, 6, fail_rank=1)
     assert [o[1] for o in out] == ["error", "error"]
     assert all("rank 1" in o[2] or "rank(s) [1]" in o[2] for o in out)
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_split_second_phase_matches_one_process(world):
+    """One integral, its leftover boxes cut into `world` contiguous shares
+    (GPUKernelquad.cu:759-768), each refined by its own rank, one
+    all-reduce: every rank gets the single-process result -- the same
+    region and evaluation counts and status, the same value and error to
+    rounding (the shares are summed in another order)."""
+    import oracle as O
+
+    fam, n, a, u, eps, cap = SPLIT_CASE
+    ref = O.Rule(n).integrate_reference(O.make_integrand(fam, n, a, u), eps, 1e-12,
+                                        phase1_cap=cap)
+    assert ref["phase2_regions"] >= world
+    out = _run(world, 0, mode="split")
+    assert [o[1] for o in out] == ["ok"] * world
+    for _, _, (value, error, nreg, neval, status) in out:
+        assert nreg == ref["nregions"] and neval == ref["neval"] and status == ref["status"]
+        assert abs(value - ref["value"]) <= 1e-12 * abs(ref["value"])
+        assert abs(error - ref["error"]) <= 1e-12 * abs(ref["value"])
+
+
+def test_split_failure_on_one_rank_reaches_all():
+    out = _run(2, 0, fail_rank=0, mode="split")
+    assert [o[1] for o in out] == ["error", "error"]
+
+
+def test_split_world_one_is_the_plain_result():
+    """Without a process group the split is the world-1 case: the oracle's
+    own two-phase result."""
+    import oracle as O
+
+    fam, n, a, u, eps, cap = SPLIT_CASE
+    ref = O.Rule(n).integrate_reference(O.make_integrand(fam, n, a, u), eps, 1e-12,
+                                        phase1_cap=cap)
+    res = P.integrate_split(_oracle_split_shard, eps, 1e-12)
+    assert (res.nregions, res.neval, res.status) == (ref["nregions"], ref["neval"],
+                                                     ref["status"])
+    assert res.integral == ref["value"] and res.error == ref["error"]
