@@ -961,7 +961,9 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
     n_left = nx.n_left;
   }
 
-  const bool shard = opt.shard_world > 1;
+  // a share of the second phase (cub_integrate_shard sets phase1_out; one
+  // share of one is the whole second phase, reported the same way)
+  const bool shard = ws.phase1_out != nullptr;
   if (status == kOk && n_left > 0 && (ws.phase1_out || shard)) {
     // the first phase's results, before the second phase adds to them
     if (!states_fresh) {
@@ -989,7 +991,7 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
     ws.phase1_out = nullptr;  // filled from the final results below
   }
   long long box0 = 0, box1 = n_left;
-  if (shard && n_left > 0) {
+  if (shard && n_left > 0 && opt.shard_world > 1) {
     const long long each = n_left / opt.shard_world;
     box0 = (long long)opt.shard_rank * each;
     box1 = opt.shard_rank == opt.shard_world - 1 ? n_left : box0 + each;
@@ -1030,6 +1032,8 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
     p.next_box = ws.counter;
     p.out = ws.left_res;
     p.ist = ws.ist;
+    // one integral's shares follow the reference's leftover order
+    p.pair_half = shard && opt.shard_world > 1 && nint == 1 ? (int)(n_left / 2) : 0;
     if (ws.timing) ws.ck(cudaEventRecord(ws.ev[2], s));
     k_phase2<N, Src><<<(unsigned)blocks, 128, 0, s>>>(src, T, p);
     if (ws.timing) ws.ck(cudaEventRecord(ws.ev[3], s));

@@ -53,6 +53,13 @@ struct Phase2Args {
   int* next_box;    // work counter
   LeftoverResult* out;
   const IntegralState* ist;
+  // 0: the counter walks the leftover list in its own order.  h > 0: the
+  // list holds the two children of h regions adjacently (2j, 2j + 1), and
+  // the counter walks it in the reference's order, first children then
+  // second children (position q < h is box 2q, q >= h is box 2(q - h) + 1),
+  // so that a contiguous range of positions is the reference's
+  // multi-device share (GPUKernelquad.cu:759-768)
+  int pair_half;
 };
 
 namespace detail {
@@ -148,6 +155,7 @@ __global__ void __launch_bounds__(128, 3) k_phase2(Src src, RuleTables T, Phase2
     if (lane == 0) box = atomicAdd(a.next_box, 1);
     box = __shfl_sync(0xffffffffu, box, 0);
     if (box >= a.n_left) break;
+    if (a.pair_half) box = box < a.pair_half ? 2 * box : 2 * (box - a.pair_half) + 1;
     const int k = a.left_rid[box];
     const IntegralState& is = a.ist[k];
     const double epsrel = is.epsrel, epsabs = is.epsabs;

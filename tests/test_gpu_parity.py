@@ -798,12 +798,11 @@ def test_replicated_kernel_bit_identical_batches(cub, ctx):
 
 @pytest.mark.parametrize("world", [1, 2, 3])
 def test_split_second_phase_matches_whole_integral(cub, oracle, ctx, world):
-    """One integral's leftover boxes cut into `world` shares
-    (cub_integrate_shard, the reference's multi-device cut), the shares run
-    one after another on this GPU and combined as the all-reduce of
-    cubature.parallel.integrate_split does: the single-call result -- the
-    same region and evaluation counts and status, the same value and error
-    to rounding -- and the oracle's shares give the same parts."""
+    """One integral's leftover boxes cut into `world` contiguous shares
+    (cub_integrate_shard), the shares run one after another on this GPU and
+    combined as the all-reduce of cubature.parallel.integrate_split does:
+    the single-call result -- the same region and evaluation counts and
+    status, the same value and error to rounding."""
     from cubature import parallel as P
 
     f = cub.Integrand("product_peak", 4, [30.0, 40.0, 20.0, 35.0], [0.3, 0.6, 0.5, 0.4])
@@ -821,13 +820,16 @@ def test_split_second_phase_matches_whole_integral(cub, oracle, ctx, world):
     assert (nreg, neval, status) == (whole.nregions, whole.neval, whole.status)
     assert abs(value - whole.integral) <= 1e-12 * abs(whole.integral)
     assert abs(error - whole.error) <= 1e-12 * abs(whole.integral)
-    # the shares of the oracle's second phase
+    # the oracle cuts its leftover list in the reference's order (first
+    # children, then second children), as the engine's shares do: the same
+    # first phase, and shares of the same boxes (regions within the heap-tie
+    # tolerance of the second phase)
     fc = oracle.make_integrand("product_peak", 4, [30.0, 40.0, 20.0, 35.0], [0.3, 0.6, 0.5, 0.4])
     for r in range(world):
         q1, qp = oracle.Rule(4).integrate_reference_shard(fc, 1e-7, 1e-12, r, world,
                                                           phase1_cap=512)
         assert q1["nregions"] == p1.nregions and qp["phase2_regions"] > 0
-        assert abs(qp["nregions"] - shares[r][1].nregions) <= 5e-3 * qp["nregions"]
+        assert abs(qp["nregions"] - shares[r][1].nregions) <= 5e-3 * qp["nregions"], r
     # world 1 through the combiner is the plain result
     if world == 1:
         res = P.integrate_split(lambda r, w: ctx.integrate_shard(f, 1e-7, 1e-12, r, w, opts),
