@@ -259,8 +259,8 @@ struct GroupSmem {
 // set-1/2 values (fst); value, error and split axis (finish_region).
 // Thread 0 of the group returns the result.  Every thread of the block must
 // call it (block barriers).
-// A set whose sums are +0.0 in every lane of a warp reduces to +0.0, so
-// its shuffle tree is skipped (same bits).
+// The nine shuffle trees run level by level, so their latencies overlap;
+// each set's tree adds in the same order as on its own.
 template <int N, int G>
 __device__ __forceinline__ RegionResult group_finish(double (&S)[kNumSets], const double (&H)[N],
                                                      const RuleTables& T,
@@ -268,15 +268,18 @@ __device__ __forceinline__ RegionResult group_finish(double (&S)[kNumSets], cons
                                                      int t) {
   constexpr int W = G / 32;
   const int lane = t & 31, wid = threadIdx.x >> 5;
+  // the Jacobian (box volume, axis order) before the barrier
+  double jac = 1;
 #pragma unroll
-  for (int k = 0; k < kNumSets; ++k) {
-    double v = S[k];
-    if (__any_sync(0xffffffffu, __double_as_longlong(v) != 0)) {
+  for (int d = 0; d < N; ++d) jac = __dmul_rn(jac, H[d]);
 #pragma unroll
-      for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-    }
-    S[k] = v;
-    if (W > 1 && lane == 0) red[wid][k] = v;
+  for (int off = 16; off > 0; off >>= 1) {
+#pragma unroll
+    for (int k = 0; k < kNumSets; ++k) S[k] += __shfl_xor_sync(0xffffffffu, S[k], off);
+  }
+  if (W > 1 && lane == 0) {
+#pragma unroll
+    for (int k = 0; k < kNumSets; ++k) red[wid][k] = S[k];
   }
   __syncthreads();
   RegionResult r;
@@ -316,12 +319,7 @@ __device__ __forceinline__ RegionResult group_finish(double (&S)[kNumSets], cons
         rs.axis = oa;
       }
     }
-    if (lane == 0) {
-      double jac = 1;
-#pragma unroll
-      for (int d = 0; d < N; ++d) jac = __dmul_rn(jac, H[d]);
-      r = finish_region<N>(rs, T, jac, 0);
-    }
+    if (lane == 0) r = finish_region<N>(rs, T, jac, 0);
   }
   __syncthreads();
   return r;

@@ -352,30 +352,45 @@ __device__ __forceinline__ void rep_decide(const RepArgs& p, RepSmem<N>& sm, int
   for (int c = threadIdx.x; c < nc; c += blockDim.x)
     sm.owner[c] = rep_slot_owner(sm.ist, nint, (long long)c * 32);
   __syncthreads();
-  if (tracer) trace_mark(p.base.ctl, it, 1);
-  for (int c = warp; c < nc; c += blockDim.x / 32) {
-    const int k = sm.owner[c];
-    const long long i = (long long)c * 32 + lane;
-    const double av = __ldcg(avg + i), er = __ldcg(err + i);
-    const bool act = er / max_err(av, sm.ist[k].epsrel, sm.ist[k].epsabs) > 1;
-    double s0 = av, s1 = er, s2 = act ? 0.0 : av, s3 = act ? 0.0 : er;
+  // a warp's chunks in batches of four: the loads of a batch are in flight
+  // together
+  constexpr int kBatch = 4;
+  const int nw = blockDim.x / 32;
+  for (int c0 = warp; c0 < nc; c0 += kBatch * nw) {
+    double avb[kBatch], erb[kBatch];
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-      s0 += __shfl_xor_sync(0xffffffffu, s0, off);
-      s1 += __shfl_xor_sync(0xffffffffu, s1, off);
-      s2 += __shfl_xor_sync(0xffffffffu, s2, off);
-      s3 += __shfl_xor_sync(0xffffffffu, s3, off);
+    for (int u = 0; u < kBatch; ++u) {
+      const long long i = (long long)(c0 + u * nw) * 32 + lane;
+      const bool in = c0 + u * nw < nc;
+      avb[u] = in ? __ldcg(avg + i) : 0.0;
+      erb[u] = in ? __ldcg(err + i) : 0.0;
     }
-    const unsigned b = __ballot_sync(0xffffffffu, act);
-    if (lane == 0) {
-      ChunkPartial q;
-      q.sum_avg = s0;
-      q.sum_err = s1;
-      q.fin_avg = s2;
-      q.fin_err = s3;
-      q.nactive = __popc(b);
-      q.mask = b;
-      sm.part[c] = q;
+#pragma unroll
+    for (int u = 0; u < kBatch; ++u) {
+      const int c = c0 + u * nw;
+      if (c >= nc) break;
+      const int k = sm.owner[c];
+      const double av = avb[u], er = erb[u];
+      const bool act = er / max_err(av, sm.ist[k].epsrel, sm.ist[k].epsabs) > 1;
+      double s0 = av, s1 = er, s2 = act ? 0.0 : av, s3 = act ? 0.0 : er;
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        s0 += __shfl_xor_sync(0xffffffffu, s0, off);
+        s1 += __shfl_xor_sync(0xffffffffu, s1, off);
+        s2 += __shfl_xor_sync(0xffffffffu, s2, off);
+        s3 += __shfl_xor_sync(0xffffffffu, s3, off);
+      }
+      const unsigned b = __ballot_sync(0xffffffffu, act);
+      if (lane == 0) {
+        ChunkPartial q;
+        q.sum_avg = s0;
+        q.sum_err = s1;
+        q.fin_avg = s2;
+        q.fin_err = s3;
+        q.nactive = __popc(b);
+        q.mask = b;
+        sm.part[c] = q;
+      }
     }
   }
   __syncthreads();
@@ -432,11 +447,13 @@ __device__ __forceinline__ void rep_decide(const RepArgs& p, RepSmem<N>& sm, int
         m += pc.nactive;
       }
     }
+    if (tracer) trace_mark(p.base.ctl, it, 1);
     bool entered = false;
     if (run) {
       decide_integral(is, s0, s1, s2, s3, m, p.base);
       entered = is.state == kStatePhase2;
     }
+    if (tracer) trace_mark(p.base.ctl, it, 6);
     const bool cont = run && is.state == kStateRunning;
     const int nextc = cont ? is.next_count : 0;
     const int vn = (nextc + 31) & ~31;
@@ -629,7 +646,6 @@ __global__ void __launch_bounds__(256, 2) k_replicated(Src src, RuleTables T, Re
       }
       if (tracer) trace_mark(ctl, it, 2);
       detail::rep_decide<N>(p, sm, st.n, par, st.n_left, it);
-      if (tracer) trace_mark(ctl, it, 6);
       const IterState nx = sm.next;
       if (nx.handoff) detail::rep_write_children<N>(p, sm, st.n, cur, par, false);
       if (nx.n_running == 0 || nx.n == 0)

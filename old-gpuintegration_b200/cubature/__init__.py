@@ -280,7 +280,19 @@ class Integrand:
     u: float | Sequence[float] = 0.5
 
     def params(self) -> GenzParams:
-        return make_params(self.ndim, self.a, self.u)
+        # built once per parameter set when a and u are hashable (scalars,
+        # tuples); lists are read afresh on every call
+        try:
+            key = (self.ndim, self.a, self.u)
+            hash(key)
+        except TypeError:
+            return make_params(self.ndim, self.a, self.u)
+        cached = self.__dict__.get("_params")
+        if cached is not None and cached[0] == key:
+            return cached[1]
+        p = make_params(self.ndim, self.a, self.u)
+        self.__dict__["_params"] = (key, p)
+        return p
 
 
 @dataclass
