@@ -341,6 +341,54 @@ def reference_gpu_rate(workload: dict, warmup: int, reps: int, device: int):
                       "integrate(), device synchronised on both sides"}
 
 
+def cv_side_block(ctx, cub, count: int, epsrel: float = 1e-6, epsabs: float = 1e-12) -> dict:
+    """The learned control variate against the plain method on the same
+    integrands (the 7-D product-peak batch, seeds 0..count-1): one pass of
+    each, timed with the device synchronised on both sides; an integral
+    counts when it converged and lies within epsrel of the analytic value."""
+    import torch
+    import oracle as O
+
+    n = 7
+    cases = product_peak_params(n, count)
+    plist = [cub.make_params(n, a, u) for a, u in cases]
+    exact = [O.exact(O.make_integrand("product_peak", n, a, u)) for a, u in cases]
+
+    def verified(res):
+        return sum(1 for r, ex in zip(res, exact)
+                   if r.status == 0 and abs(r.integral - ex) <= epsrel * abs(ex))
+
+    out = {"workload": "cv_productpeak_7d_batch", "integrals": count, "epsrel": epsrel,
+           "epsabs": epsabs, "target_ratio": 3.0}
+    try:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res_cv, st = ctx.cv_integrate_batch("product_peak", plist, epsrel, epsabs)
+        torch.cuda.synchronize()
+        t_cv = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        res_pl = ctx.integrate_batch("product_peak", n, plist, epsrel, epsabs,
+                                     cub.options(policy=cub.POLICY_BREADTH))
+        torch.cuda.synchronize()
+        t_pl = time.perf_counter() - t0
+    except Exception as e:  # reported, the headline line still prints
+        out["error"] = f"{type(e).__name__}: {e}"
+        return out
+    g_cv, g_pl = verified(res_cv), verified(res_pl)
+    out["cv"] = {"value": g_cv / t_cv, "unit": "integrals/s", "seconds": t_cv, "verified": g_cv,
+                 "regions": int(sum(r.nregions for r in res_cv)),
+                 "fallbacks": int(st["fallbacks"]), "rejected": int(st["rejected"]),
+                 "mean_residual_ratio": st["mean_residual_ratio"],
+                 "ms_coarse": st["ms_coarse"], "ms_train": st["ms_train"],
+                 "ms_integrate": st["ms_integrate"],
+                 "regions_residual": int(st["regions_residual"]),
+                 "regions_network": int(st["regions_network"])}
+    out["plain"] = {"value": g_pl / t_pl, "unit": "integrals/s", "seconds": t_pl,
+                    "verified": g_pl, "regions": int(sum(r.nregions for r in res_pl))}
+    out["ratio"] = out["cv"]["value"] / out["plain"]["value"] if out["plain"]["value"] else None
+    return out
+
+
 def cpu_sample_text(workload: dict, done: int, el: float,
                     regions_per_integral: float | None = None) -> str:
     if "tables" in workload:
@@ -393,6 +441,11 @@ def main() -> int:
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true",
                     help="skip timing the reference engine on the GPU beside the run")
+    ap.add_argument("--no-cv", action="store_true",
+                    help="skip the learned-control-variate side block of the default workload")
+    ap.add_argument("--cv-count", type=int, default=64,
+                    help="integrals of the control-variate side block (the first of the "
+                         "256-integral configuration; --cv-count 256 runs all of it)")
     ap.add_argument("--count", type=int, default=0,
                     help="batch workloads: integrals per step (default: the workload's)")
     args = ap.parse_args()
@@ -533,7 +586,6 @@ def main() -> int:
     torch.cuda.synchronize()
 
     ctx.reset_stats()
-    ctx.set_timing(True)
     step_ms, wall_ms = [], []
     results = None
     with ClockSampler(local) as clocks:
@@ -552,8 +604,25 @@ def main() -> int:
             torch.cuda.synchronize()
             step_ms.append(ev0.elapsed_time(ev1))
             wall_ms.append((t1 - t0) * 1e3)
-    ctx.set_timing(False)
     st = ctx.stats()
+    # Kernel durations for the roofline: the same steps again with the
+    # library's CUDA events around every launch (counters reset).  Timing
+    # makes the library wait for each launch with a stream synchronisation
+    # instead of its completion word, so `value` and `e2e` come from the
+    # untimed pass above.
+    ctx.reset_stats()
+    ctx.set_timing(True)
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        if pg:
+            pg.barrier()
+        step()
+        torch.cuda.synchronize()
+    ctx.set_timing(False)
+    st_timed = ctx.stats()
+    for key in ("ms_persistent", "ms_eval", "ms_phase2"):
+        st[key] = st_timed[key]
     plain_cmp = None
     single_cmp = None
     if "items" in workload and len(workload["items"]) > 1 and same_dim:
@@ -679,6 +748,9 @@ def main() -> int:
                "sample": cpu_sample_text(workload, done, el, per), "cpu_model": cpu_model(),
                "one_thread": {"value": rate1, "unit": "integrals/s", "cores": 1,
                               "sample": cpu_sample_text(workload, done1, el1, per)}}
+    cv_side = None
+    if rank == 0 and "items" in workload and not args.no_cv and args.cv_count > 0:
+        cv_side = cv_side_block(ctx, cub, args.cv_count)
     ref_gpu = None
     if rank == 0 and not args.no_ref_gpu:
         ref_gpu = reference_gpu_rate(workload, 3, max(5, args.steps), local)
@@ -699,7 +771,8 @@ def main() -> int:
                        "timing": "value: CUDA events on the library's stream around each "
                                  "step's public-API calls (inputs are parameter blocks; the "
                                  "host drives the launches); e2e: host wall clock around "
-                                 "the same calls"},
+                                 "the same calls; roofline kernel times: a second pass of "
+                                 "the same steps with the library's per-launch events on"},
             "geval_per_s": world * neval * args.steps / (dev_ms / 1e3) / 1e9,
             "e2e": {"value": e2e_value, "unit": "integrals/s",
                     "h2d_bytes_per_step": st.get("h2d_bytes", 0) // max(1, args.steps),
@@ -730,6 +803,8 @@ def main() -> int:
         }
         if ref_gpu is not None:
             line["reference_gpu"] = ref_gpu
+        if cv_side is not None:
+            line["cv_vs_plain"] = cv_side
         if plain_cmp is not None:
             line["plain_same_integrands"] = plain_cmp
         if single_cmp is not None:

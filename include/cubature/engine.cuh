@@ -116,6 +116,10 @@ class Workspace {
 
   // Free every device and pinned buffer; the next run reserves afresh.
   void release() {
+    drop_launch_graphs();
+    if (done_host_) cudaFreeHost(done_host_);
+    done_host_ = nullptr;
+    done_dev_ = nullptr;
     for (auto& p : bufs_)
       if (p.first) cudaFree(p.first);
     bufs_.clear();
@@ -405,6 +409,7 @@ class Workspace {
     ist_host_ = reinterpret_cast<IntegralState*>(static_cast<char*>(host_block_) + kStateOffset);
     if (!ck(cudaMemsetAsync(ctl, 0, sizeof(Control), s))) return false;
     if (!ck(cudaMemsetAsync(int_cnt, 0, sizeof(unsigned) * n, s))) return false;
+    barrier_clean = true;
     nint_cap_ = n;
     return true;
   }
@@ -434,6 +439,137 @@ class Workspace {
       return false;
     }
     return true;
+  }
+
+  // The device control block's barrier counters are zero: set when the
+  // block is cleared or uploaded and after a replicated launch (its last
+  // block zeroes them), cleared after a launch of the persistent kernel.
+  bool barrier_clean = true;
+
+  // Completion word of replicated launches: a mapped pinned word that the
+  // kernel sets to the launch's sequence number after storing its final
+  // states in the pinned block, so the host stops waiting then, not when
+  // the whole grid has retired.  Null when mapped memory is unavailable.
+  unsigned* done_word() {
+    if (!done_host_ && !done_failed_) {
+      if (cudaHostAlloc(reinterpret_cast<void**>(&done_host_), 64, cudaHostAllocMapped) !=
+              cudaSuccess ||
+          cudaHostGetDevicePointer(reinterpret_cast<void**>(&done_dev_), done_host_, 0) !=
+              cudaSuccess) {
+        if (done_host_) cudaFreeHost(done_host_);
+        done_host_ = nullptr;
+        done_dev_ = nullptr;
+        done_failed_ = true;
+        cudaGetLastError();
+      } else {
+        *done_host_ = 0;
+      }
+    }
+    return done_dev_;
+  }
+  unsigned next_seq() {
+    if (++done_seq_ == 0) ++done_seq_;
+    return done_seq_;
+  }
+
+  // Wait until the completion word holds seq.  The stream is queried now
+  // and then, so a launch that failed (or finished without storing) ends
+  // the wait with its error instead of spinning.
+  bool wait_done(unsigned seq, cudaStream_t s) {
+    for (unsigned i = 1;; ++i) {
+      if (__atomic_load_n(done_host_, __ATOMIC_ACQUIRE) == seq) return true;
+      if ((i & 4095) == 0) {
+        const cudaError_t e = cudaStreamQuery(s);
+        if (e == cudaErrorNotReady) continue;
+        if (e != cudaSuccess) return ck(e);
+        if (__atomic_load_n(done_host_, __ATOMIC_ACQUIRE) == seq) return true;
+        err_ = "replicated launch finished without storing its states";
+        return false;
+      }
+    }
+  }
+
+  // One replicated launch as a replay: the upload of `bytes` bytes of the
+  // pinned control block and states (none when bytes is 0: the launch
+  // carries its starting states), then the cooperative launch of `func`
+  // on `blocks` blocks of 256 threads with `args`.  The two are captured
+  // into a CUDA graph on first use, and again when the kernel, the grid or
+  // the copy changes; later calls set the kernel node's arguments and
+  // launch the graph, which costs the host less than a copy plus a
+  // cooperative launch.  Returns false on a CUDA error; a capture that is
+  // not possible here (the stream is being captured by the caller, say)
+  // falls back to the copy and launch.
+  bool launch_replicated(const void* func, unsigned blocks, void** args, size_t bytes,
+                         cudaStream_t s) {
+    // one graph per kernel and copy, so that calls alternating between
+    // integrands reuse theirs (the oldest of kLaunchGraphs is dropped)
+    LaunchGraph* gp = nullptr;
+    for (auto& e : lg_)
+      if (e.exec && e.func == func && e.blocks == blocks && e.bytes == bytes && e.dst == ctl &&
+          e.src == ctl_host_)
+        gp = &e;
+    if (!gp) {
+      gp = &lg_[0];
+      for (auto& e : lg_)
+        if (!e.exec || e.used < gp->used) gp = &e;
+      drop_launch_graph(*gp);
+    }
+    LaunchGraph& g = *gp;
+    g.used = ++lg_clock_;
+    if (!g.exec && !graph_failed_) {
+      cudaGraph_t graph = nullptr;
+      cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+      if (e == cudaSuccess) {
+        cudaError_t e1 = bytes ? cudaMemcpyAsync(ctl, ctl_host_, bytes, cudaMemcpyHostToDevice, s)
+                               : cudaSuccess;
+        if (e1 == cudaSuccess)
+          e1 = cudaLaunchCooperativeKernel(func, dim3(blocks), dim3(256), args, 0, s);
+        e = cudaStreamEndCapture(s, &graph);
+        if (e == cudaSuccess) e = e1;
+      }
+      cudaGraphNode_t knode = nullptr;
+      if (e == cudaSuccess) {
+        size_t nn = 0;
+        e = cudaGraphGetNodes(graph, nullptr, &nn);
+        std::vector<cudaGraphNode_t> nodes(nn);
+        if (e == cudaSuccess) e = cudaGraphGetNodes(graph, nodes.data(), &nn);
+        for (size_t i = 0; e == cudaSuccess && i < nn; ++i) {
+          cudaGraphNodeType t;
+          if (cudaGraphNodeGetType(nodes[i], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel)
+            knode = nodes[i];
+        }
+      }
+      if (e == cudaSuccess && knode) e = cudaGraphInstantiate(&g.exec, graph, 0);
+      if (e != cudaSuccess || !knode || !g.exec) {
+        if (graph) cudaGraphDestroy(graph);
+        g.exec = nullptr;
+        graph_failed_ = true;
+        cudaGetLastError();
+      } else {
+        g.graph = graph;
+        g.kernel = knode;
+        g.func = func;
+        g.blocks = blocks;
+        g.bytes = bytes;
+        g.dst = ctl;
+        g.src = ctl_host_;
+        // the recorded launch holds this call's arguments already
+        return ck(cudaGraphLaunch(g.exec, s));
+      }
+    }
+    if (!g.exec) {
+      return (!bytes || ck(cudaMemcpyAsync(ctl, ctl_host_, bytes, cudaMemcpyHostToDevice, s))) &&
+             ck(cudaLaunchCooperativeKernel(func, dim3(blocks), dim3(256), args, 0, s));
+    }
+    cudaKernelNodeParams kp = {};
+    kp.func = const_cast<void*>(func);
+    kp.gridDim = dim3(blocks);
+    kp.blockDim = dim3(256);
+    kp.sharedMemBytes = 0;
+    kp.kernelParams = args;
+    kp.extra = nullptr;
+    return ck(cudaGraphExecKernelNodeSetParams(g.exec, g.kernel, &kp)) &&
+           ck(cudaGraphLaunch(g.exec, s));
   }
 
   size_t bytes_reserved() const { return bytes_; }
@@ -472,15 +608,50 @@ class Workspace {
   void* ctl_block_ = nullptr;
   void* host_block_ = nullptr;
   void* host_block_dev_ = nullptr;  // device address of host_block_ (mapped)
+  // the graphs of launch_replicated and what each was recorded for
+  struct LaunchGraph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaGraphNode_t kernel = nullptr;
+    const void* func = nullptr;
+    unsigned blocks = 0;
+    size_t bytes = 0;
+    const void* dst = nullptr;
+    const void* src = nullptr;
+    unsigned long long used = 0;  // lg_clock_ at the last use
+  };
+  static constexpr int kLaunchGraphs = 8;
+  LaunchGraph lg_[kLaunchGraphs];
+  unsigned long long lg_clock_ = 0;
+  bool graph_failed_ = false;
+  static void drop_launch_graph(LaunchGraph& g) {
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    if (g.graph) cudaGraphDestroy(g.graph);
+    g = LaunchGraph();
+  }
+  void drop_launch_graphs() {
+    for (auto& g : lg_) drop_launch_graph(g);
+  }
+  unsigned* done_host_ = nullptr;  // completion word (pinned, mapped)
+  unsigned* done_dev_ = nullptr;
+  unsigned done_seq_ = 0;
+  bool done_failed_ = false;
   size_t bytes_ = 0;
   std::string err_;
   Stats stats_;
 };
 
 inline int sm_count(int device) {
-  int n = 0;
+  // queried once per device (every call needs it)
+  static std::atomic<int> cache[64];
+  const int d = device >= 0 && device < 64 ? device : 0;
+  int n = cache[d].load(std::memory_order_relaxed);
+  if (n > 0 && device == d) return n;
+  n = 0;
   cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, device);
-  return n > 0 ? n : 148;
+  n = n > 0 ? n : 148;
+  if (device == d) cache[d].store(n, std::memory_order_relaxed);
+  return n;
 }
 
 // Region-list capacity when the caller leaves it to the library: the slots
@@ -694,6 +865,11 @@ inline RepArgs rep_args(const Workspace& ws, const EngineArgs& a, const Options&
   p.host_words = 0;
   p.spin_limit = opt.barrier_spins > 0 ? opt.barrier_spins : detail::kBarrierSpins;
   p.hold_block = opt.hold_block;
+  p.done = nullptr;
+  p.seq = 0;
+  p.param_state = 0;
+  p.cur0 = 0;
+  std::memset(&p.host0, 0, sizeof(p.host0));
   return p;
 }
 
@@ -710,6 +886,7 @@ inline void persistent_control(Workspace& ws, const IterState& hs, int cur) {
   ws.ctl_host_->cur = cur;
   ws.ctl_host_->done_cnt = 0;
   ws.ctl_host_->bar_count = 0;
+  ws.ctl_host_->exit_count = 0;
   ws.ctl_host_->timeout = 0;
   ws.ctl_host_->exit_reason = 0;
   std::memset(ws.ctl_host_->trace, 0, sizeof(ws.ctl_host_->trace));
@@ -831,7 +1008,14 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
         st.d2h_bytes += (long long)(sizeof(IntegralState) * nint);
         detail::persistent_control(ws, hs, cur);
       }
-      if (!ws.ck(cudaMemcpyAsync(ws.ctl, ws.ctl_host_, up, cudaMemcpyHostToDevice, s)))
+      // small batches on the replicated kernel: the upload and the launch
+      // replayed from a graph, and the wait ends when the kernel has stored
+      // its states (launch_replicated, wait_done)
+      const bool fast = use_rep && !ws.timing && ws.direct_states(nint) && ws.done_word();
+      // a batch of up to kParamStates integrals passes its starting states
+      // with the launch when the barrier counters are known to be zero
+      const bool pstate = fast && nint <= kParamStates && ws.barrier_clean;
+      if (!fast && !ws.ck(cudaMemcpyAsync(ws.ctl, ws.ctl_host_, up, cudaMemcpyHostToDevice, s)))
         return kErrCuda;
       uploaded = true;
       st.h2d_bytes += (long long)up;
@@ -841,15 +1025,31 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
       if (count_regions)
         for (int k = 0; k < nint; ++k) nreg_before[k] = h[k].nregions;
       if (ws.timing) ws.ck(cudaEventRecord(ws.ev[0], s));
+      unsigned seq = 0;  // completion word value of a fast launch
       if (use_rep) {
         RepArgs p = detail::rep_args(ws, a, opt, c0.iters_done, rmax, grid_pending, dv, per,
                                      padded, d_box);
         p.host_out = ws.direct_states(nint);
         p.host_words = (int)(ws.state_bytes(nint) / 8);
+        if (fast) {
+          p.done = ws.done_word();
+          p.seq = seq = ws.next_seq();
+        }
+        if (pstate) {
+          p.param_state = 1;
+          p.cur0 = cur;
+          p.host0 = hs;
+          for (int k = 0; k < nint; ++k) p.ist0[k] = h[k];
+        }
         void* args[] = {(void*)&src, (void*)&T, (void*)&p};
-        if (!ws.ck(cudaLaunchCooperativeKernel((const void*)k_replicated<N, Src>,
-                                               dim3(rblocks), dim3(256), args, 0, s)))
+        if (fast) {
+          if (!ws.launch_replicated((const void*)k_replicated<N, Src>, (unsigned)rblocks, args,
+                                    pstate ? 0 : up, s))
+            return kErrCuda;
+        } else if (!ws.ck(cudaLaunchCooperativeKernel((const void*)k_replicated<N, Src>,
+                                                      dim3(rblocks), dim3(256), args, 0, s))) {
           return kErrCuda;
+        }
       } else {
         PersistArgs p = detail::persist_args(ws, a, opt, c0.iters_done, pmax, grid_pending, dv,
                                              per, padded, d_box);
@@ -861,6 +1061,7 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
           return kErrCuda;
       }
       grid_pending = false;
+      ws.barrier_clean = use_rep;
       if (ws.timing) ws.ck(cudaEventRecord(ws.ev[1], s));
       st.launches += 1;
       st.persistent_launches += 1;
@@ -871,7 +1072,11 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
           !ws.ck(cudaMemcpyAsync(ws.ctl_host_, ws.ctl, ws.state_bytes(nint),
                                  cudaMemcpyDeviceToHost, s)))
         return kErrCuda;
-      if (!ws.ck(cudaStreamSynchronize(s))) return kErrCuda;
+      if (seq) {
+        if (!ws.wait_done(seq, s)) return kErrCuda;
+      } else if (!ws.ck(cudaStreamSynchronize(s))) {
+        return kErrCuda;
+      }
       st.d2h_bytes += (long long)ws.state_bytes(nint);
       states_fresh = true;
       if (ws.timing) {

@@ -90,7 +90,7 @@ struct Control {
   int pad;
   unsigned done_cnt;   // integrals decided in this iteration
   unsigned bar_count;  // grid barrier arrivals since the launch (monotonic)
-  unsigned bar_gen;    // unused
+  unsigned exit_count;  // replicated kernel: blocks that have left this launch
   int timeout;         // a bounded wait gave up
   // globaltimer stamps (ns) of the persistent kernels' first kTraceIters
   // iterations, kTraceSlots per iteration (diagnostics, read back with the
@@ -98,9 +98,9 @@ struct Control {
   // 2 grid barrier passed, 3 decider read its integral state, 4 block 0's
   // evaluations done, 5 last chunk summed, 6 integrals decided, 7 chunk sums
   // combined.  Replicated kernel (block 0): 0 start, 7 first region set up,
-  // 4 evaluations done, 2 grid barrier passed, 1 chunk owners found,
-  // 3 chunk partials formed, 5 integrals decided (warp 0), 6 decision
-  // visible to the block.
+  // 4 evaluations done, 2 grid barrier passed, 3 chunk partials formed,
+  // 1 per-integral sums formed (warp 0), 6 stop decision taken, 5 next
+  // segments assigned.
   unsigned long long trace[64];
 };
 constexpr int kTraceIters = 8;

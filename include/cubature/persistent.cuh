@@ -92,13 +92,19 @@ __device__ __forceinline__ void red_release_add(unsigned* p, unsigned v) {
 
 // Grid-wide barrier on a monotonic arrival counter: the b-th barrier of a
 // launch (b = 1, 2, ...) waits for b * gridDim.x arrivals.  Bounded wait
-// (spin_limit polls); returns false once any block gave up waiting (all
-// blocks then return).  A block with arrive == false waits without
+// (spin_limit polls); returns false when this block gave up waiting or saw
+// that another block did (every block then returns: a block that passed
+// this barrier meets the next one without the one that gave up).  A block
+// with arrive == false waits without
 // arriving: the failure-detection tests use it to make every wait run out.
 // Ordering needs no separate fences: the block's writes precede thread 0's
 // gpu-scope release through the CTA barrier, the release and acquire
 // operations are cumulative, and the closing CTA barrier orders the
 // block's later reads after thread 0's acquire.
+// Only the arrival counter is read on the way through: the shared timeout
+// flag is read every 64th poll, so a block that gave up is noticed within
+// 64 polls (at the latest at the next barrier, which it does not reach),
+// and a passing wait costs one acquire load after the last arrival.
 __device__ __forceinline__ bool grid_barrier(Control* ctl, unsigned target, long long spin_limit,
                                              bool arrive) {
   __shared__ int ok;
@@ -108,14 +114,14 @@ __device__ __forceinline__ bool grid_barrier(Control* ctl, unsigned target, long
     long long spins = 0;
     int good = 1;
     while (ld_acquire(&ctl->bar_count) < target) {
-      if (++spins > spin_limit || *(volatile int*)&ctl->timeout) {
+      if ((++spins & 63) == 0 && (spins > spin_limit || *(volatile int*)&ctl->timeout)) {
         atomicExch(&ctl->timeout, 1);
         good = 0;
         break;
       }
       __nanosleep(32);
     }
-    ok = good && *(volatile int*)&ctl->timeout == 0;
+    ok = good;
   }
   __syncthreads();
   return ok;
@@ -247,6 +253,7 @@ constexpr bool kTwoPointsInFlight<MixedGenz<M>> = false;
 template <int N>
 struct GroupSmem {
   PointTable<N> pt;
+  RuleTables tables;  // stage_tables copy of the kernel's tables
   double red[8][kNumSets];      // one row per warp of the block
   double fstage[8][4 * N + 1];  // centre and set-1/2 values, per group
   int flag[8];
@@ -256,7 +263,8 @@ struct GroupSmem {
 // The set sums of the G threads of a group (S, per thread) combined into
 // the region's result: warp shuffle trees, then the warps' partials in
 // warp order; the fourth difference per axis from the staged centre and
-// set-1/2 values (fst); value, error and split axis (finish_region).
+// set-1/2 values (fst); value, error and split axis (finish_region's
+// arithmetic, spread over five lanes).
 // Thread 0 of the group returns the result.  Every thread of the block must
 // call it (block barriers).
 // The nine shuffle trees run level by level, so their latencies overlap;
@@ -319,10 +327,53 @@ __device__ __forceinline__ RegionResult group_finish(double (&S)[kNumSets], cons
         rs.axis = oa;
       }
     }
-    if (lane == 0) r = finish_region<N>(rs, T, jac, 0);
+    // Value and error on five lanes: lane q forms rule q's sum, lanes 1-3
+    // the null-rule errors, each with finish_region's arithmetic for its
+    // rule (same operations, same order, so the same bits).  T is read by
+    // lane index, so it must be a shared-memory copy (stage_tables).
+    double sq = 0;
+    if (lane < kNumRules) {
+      double acc = 0;
+#pragma unroll
+      for (int k = 0; k < kNumSets; ++k) acc = __dadd_rn(acc, __dmul_rn(T.wt[k][lane], rs.S[k]));
+      sq = __dmul_rn(acc, jac);
+    }
+    const double sq1 = __shfl_down_sync(0xffffffffu, sq, 1);
+    double nq = 0;
+    if (lane >= 1 && lane < kNumRules - 1) {
+      double m = 0;
+#pragma unroll
+      for (int k = 0; k < kNumSets; ++k) {
+        const double e =
+            __dmul_rn(fabs(__dadd_rn(sq1, __dmul_rn(T.scale[k][lane], sq))), T.norm[k][lane]);
+        m = (m > e) ? m : e;
+      }
+      nq = m;
+    }
+    const double n1 = __shfl_sync(0xffffffffu, nq, 1);
+    const double n2 = __shfl_sync(0xffffffffu, nq, 2);
+    const double n3 = __shfl_sync(0xffffffffu, nq, 3);
+    if (lane == 0) {
+      const double m12 = n1 > n2 ? n1 : n2;
+      const double m123 = m12 > n3 ? m12 : n3;
+      r.avg = sq;
+      r.err = (__dmul_rn(5.0, n1) <= n2 && __dmul_rn(5.0, n2) <= n3) ? n1 : __dmul_rn(5.0, m123);
+      r.axis = rs.axis >= 0 ? rs.axis : 0;
+    }
   }
   __syncthreads();
   return r;
+}
+
+// Copy of the rule tables in shared memory, for group_finish (which reads
+// them by lane index).  Every thread of the block calls it; a block
+// barrier must follow before the copy is read.
+__device__ __forceinline__ void stage_tables(const RuleTables& T, RuleTables& dst) {
+  static_assert(sizeof(RuleTables) % 8 == 0, "tables are copied as 8-byte words");
+  constexpr int kW = sizeof(RuleTables) / 8;
+  const unsigned long long* src = reinterpret_cast<const unsigned long long*>(&T);
+  unsigned long long* d = reinterpret_cast<unsigned long long*>(&dst);
+  for (int i = threadIdx.x; i < kW; i += blockDim.x) d[i] = src[i];
 }
 
 // One region evaluated by the G threads of group g, one point per thread
@@ -895,7 +946,7 @@ __device__ __forceinline__ void eval_step(const Src& src, const RuleTables& T, c
     {
       // groups without a region evaluate no point but join the barriers
       const auto f = src.get(k >= 0 ? k : 0);
-      const RegionResult r = eval_region_group<N, G>(f, L, H, T, sm, g, t, k >= 0);
+      const RegionResult r = eval_region_group<N, G>(f, L, H, sm.tables, sm, g, t, k >= 0);
       if (t == 0 && k >= 0) store_result(a, slot, r, epsrel, epsabs);
     }
     if (t == 0 && live) {
@@ -925,6 +976,7 @@ __global__ void __launch_bounds__(256, 2) k_persistent(Src src, RuleTables T, Pe
   __shared__ detail::Stage sg;
   __shared__ EngineArgs sargs;
   sm.pt.fill(threadIdx.x, blockDim.x);
+  detail::stage_tables(T, sm.tables);
   __syncthreads();
   Control* ctl = p.base.ctl;
   int cur = ctl->cur;

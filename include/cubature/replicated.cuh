@@ -43,6 +43,9 @@ namespace cubature {
 
 // Longest list the replicated kernel keeps (32 * kRepChunks slots).
 constexpr int kRepChunks = 128;
+// Batches up to this many integrals can start from states passed with the
+// launch (RepArgs::param_state) instead of an upload.
+constexpr int kParamStates = 4;
 
 struct RepArgs {
   EngineArgs base;  // states, tolerances, policy, capacities, leftovers
@@ -62,6 +65,20 @@ struct RepArgs {
   int host_words;
   long long spin_limit;  // grid-barrier polls before giving up
   int hold_block;        // failure-detection tests: this block never arrives (-1: none)
+  // mapped pinned word that block 0 sets to `seq` once host_out is
+  // complete, so the host can stop waiting before the grid has retired
+  // (null: the host synchronises the stream)
+  unsigned* done;
+  unsigned seq;
+  // param_state != 0: the launch starts from host0, cur0 and ist0[0..nint)
+  // instead of the control block and states in device memory (no upload
+  // before the launch; nint <= kParamStates).  The barrier counters must
+  // then be zero on entry, which the last block of every launch of this
+  // kernel leaves them.
+  int param_state;
+  int cur0;
+  IterState host0;
+  IntegralState ist0[kParamStates];
 };
 
 namespace detail {
@@ -196,6 +213,7 @@ struct RepSmem {
   int entered[kSmallBatch];         // handed to phase 2 by the last decision
   IterState next;                   // sizes of the next list
   double box[8][2 * N];             // region of each group: lower corner, widths
+  RuleTables tables;                // stage_tables copy of the kernel's tables
   int slot_k[8];                    // its integral (-1: padding or past the end)
 };
 
@@ -447,6 +465,10 @@ __device__ __forceinline__ void rep_decide(const RepArgs& p, RepSmem<N>& sm, int
         m += pc.nactive;
       }
     }
+    // The two timestamps around the decision are volatile asm, which the
+    // compiler does not move code across.  Without them it interleaved the
+    // decision with the sums above, and this warp's section took ~6 us per
+    // iteration instead of ~1 us (8-D corner peak, measured on a B200).
     if (tracer) trace_mark(p.base.ctl, it, 1);
     bool entered = false;
     if (run) {
@@ -581,17 +603,26 @@ __global__ void __launch_bounds__(256, 2) k_replicated(Src src, RuleTables T, Re
   const int nint = p.base.nint;
   Control* ctl = p.base.ctl;
   sm.tb.fill(threadIdx.x, blockDim.x);
-  for (int q = threadIdx.x; q < nint; q += blockDim.x) sm.ist[q] = p.base.ist[q];
+  detail::stage_tables(T, sm.tables);
   IterState st;
-  {
+  int cur;
+  if (p.param_state) {
+    for (int q = threadIdx.x; q < nint; q += blockDim.x) sm.ist[q] = p.ist0[q];
+    st = p.host0;
+    cur = p.cur0;
+    // the trace rows describe this launch only
+    if (blockIdx.x == 0)
+      for (int i = threadIdx.x; i < kTraceIters * kTraceSlots; i += blockDim.x) ctl->trace[i] = 0;
+  } else {
+    for (int q = threadIdx.x; q < nint; q += blockDim.x) sm.ist[q] = p.base.ist[q];
     volatile IterState* v = &ctl->host;
     st.n = v->n;
     st.n_running = v->n_running;
     st.n_left = v->n_left;
-    st.overflow = 0;
-    st.handoff = 0;
+    cur = ctl->cur;
   }
-  int cur = ctl->cur;
+  st.overflow = 0;
+  st.handoff = 0;
   __syncthreads();
   const bool tracer = blockIdx.x == 0 && threadIdx.x == 0;
   const long long ncap = p.base.ncap;
@@ -632,10 +663,10 @@ __global__ void __launch_bounds__(256, 2) k_replicated(Src src, RuleTables T, Re
       const long long per_block = (st.n + gridDim.x - 1) / gridDim.x;
       const int r = per_block <= 1 ? 1 : (per_block <= 2 ? 2 : (per_block <= 4 ? 4 : 8));
       switch (r < p.max_r ? r : p.max_r) {
-        case 1: detail::rep_eval_step<N, 256>(src, T, p, sm, mode, st.n, cur, par, it); break;
-        case 2: detail::rep_eval_step<N, 128>(src, T, p, sm, mode, st.n, cur, par, it); break;
-        case 4: detail::rep_eval_step<N, 64>(src, T, p, sm, mode, st.n, cur, par, it); break;
-        default: detail::rep_eval_step<N, 32>(src, T, p, sm, mode, st.n, cur, par, it); break;
+        case 1: detail::rep_eval_step<N, 256>(src, sm.tables, p, sm, mode, st.n, cur, par, it); break;
+        case 2: detail::rep_eval_step<N, 128>(src, sm.tables, p, sm, mode, st.n, cur, par, it); break;
+        case 4: detail::rep_eval_step<N, 64>(src, sm.tables, p, sm, mode, st.n, cur, par, it); break;
+        default: detail::rep_eval_step<N, 32>(src, sm.tables, p, sm, mode, st.n, cur, par, it); break;
       }
       if (tracer) trace_mark(ctl, it, 4);
       ++barriers;
@@ -683,6 +714,27 @@ __global__ void __launch_bounds__(256, 2) k_replicated(Src src, RuleTables T, Re
       const unsigned long long* s = reinterpret_cast<const unsigned long long*>(ctl);
       unsigned long long* dst = reinterpret_cast<unsigned long long*>(p.host_out);
       for (int i = threadIdx.x; i < p.host_words; i += blockDim.x) dst[i] = s[i];
+      if (p.done) {
+        // the block's stores to host_out, then the sequence number, at
+        // system scope
+        __syncthreads();
+        if (threadIdx.x == 0) {
+          __threadfence_system();
+          asm volatile("st.release.sys.global.u32 [%0], %1;" ::"l"(p.done), "r"(p.seq) : "memory");
+        }
+      }
+    }
+  }
+  // The last block to leave zeroes the barrier counters for the next launch
+  // (every other block has passed its last barrier by then; block 0 has
+  // stored the control block first).
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(&ctl->exit_count, 1u) == gridDim.x - 1) {
+      ctl->bar_count = 0;
+      ctl->timeout = 0;
+      ctl->exit_count = 0;
     }
   }
 }

@@ -102,7 +102,8 @@ def test_control_variate_is_correct_and_measured(cub, oracle, ctx):
     """The learned control variate (network trained on the tensor cores,
     integral of f - g plus integral of g) gives the analytic integral to the
     requested tolerance; its cost is measured against the plain method on
-    the same integrands (region counts; the gain may be below 1)."""
+    the same integrands, and the gain is asserted: fewer regions, and a time
+    ratio above a stated floor (it is below 1)."""
     import time
 
     n, eps, count = 7, 1e-4, 4
@@ -126,3 +127,11 @@ def test_control_variate_is_correct_and_measured(cub, oracle, ctx):
     plain_regions = sum(r.nregions for r in plain)
     print(f"control variate: {st}; regions cv {cv_regions} plain {plain_regions}; "
           f"time cv {t_cv:.3f} s plain {t_plain:.3f} s")
+    # What the trained network gains on these integrands: every integral
+    # takes the control-variate route, and f - g plus g needs fewer regions
+    # than f alone (measured ~1.15x).  In time it loses: the network costs
+    # far more per rule node than the integrand (measured ~0.04x); the bound
+    # below only guards against a collapse of the route.
+    assert st["fallbacks"] == 0
+    assert plain_regions / cv_regions >= 1.0, (plain_regions, cv_regions)
+    assert t_plain / t_cv >= 0.005, (t_plain, t_cv)
