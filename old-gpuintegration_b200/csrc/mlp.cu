@@ -766,6 +766,7 @@ int cv_run(cub_ctx* ctx, int count, const GenzParams* h, double epsrel, double e
   st->fallbacks = 0;
   st->rejected = 0;
   double rho_sum = 0;
+  std::vector<int> plain_idx;  // integrals the plain method integrates
   for (int k = 0; k < count; ++k) {
     double num = 0, den = 0;
     for (long long q = 0; q < S; ++q) {
@@ -783,10 +784,11 @@ int cv_run(cub_ctx* ctx, int count, const GenzParams* h, double epsrel, double e
       detail::SingleSource<F> dummy{f};
       const double half = 0.5 * tol, zero = 0.0;
       Result rr, rg;
-      // a residual that does not converge stops at this list length and
-      // the plain method takes over
+      // a residual that does not converge within 2^20 regions (its error
+      // estimate has not shrunk to the budget) stops there and the plain
+      // method takes over
       Options oc = o;
-      oc.max_slots = std::min<long long>(o.max_slots, 1ll << 22);
+      oc.max_slots = std::min<long long>(o.max_slots, 1ll << 20);
       CvHook<F> hr{net, k, f, 1.0, -1.0, half, T, sms, &scratch};
       CvHook<F> hgk{net, k, f, 0.0, 1.0, half, T, sms, &scratch};
       int r1 = run_batch<kCvDim>(ws, dummy, 1, &zero, &half, oc, &rr, s, nullptr, hr);
@@ -819,17 +821,41 @@ int cv_run(cub_ctx* ctx, int count, const GenzParams* h, double epsrel, double e
       }
     }
     if (use_plain) {
+      // integrated with the other fallbacks in one batch below
       st->fallbacks += 1;
-      detail::SingleSource<F> src{F::load(h[k])};
-      const int r = run_batch<kCvDim>(ws, src, 1, &epsrel, &epsabs, o, &cv, s);
-      if (r != kOk && r != kErrCapacity) {
-        scratch.release();
-        return engine_status(ctx, r);
-      }
+      plain_idx.push_back(k);
+      continue;
     }
     result_to_c(cv, &out[k]);
   }
   scratch.release();
+  if (!plain_idx.empty()) {
+    // the plain method on every integral that fell back, batched as
+    // cub_integrate_batch would run them (groups on consecutive parameter
+    // blocks of a staging copy)
+    const int np = (int)plain_idx.size();
+    GenzParams* d_sub = nullptr;
+    if (cudaMalloc(&d_sub, sizeof(GenzParams) * np) != cudaSuccess)
+      return cuda_error(cudaErrorMemoryAllocation, "fallback params");
+    std::unique_ptr<GenzParams, decltype(&cudaFree)> sub_guard(d_sub, cudaFree);
+    std::vector<GenzParams> hp;
+    std::vector<double> per, pea;
+    std::vector<Result> pres;
+    const int rc = grouped_batch(np, o, [&](const std::vector<int>& idx, Result* g) {
+      const int gn = (int)idx.size();
+      hp.resize(gn);
+      per.assign(gn, epsrel);
+      pea.assign(gn, epsabs);
+      for (int j = 0; j < gn; ++j) hp[j] = h[plain_idx[idx[j]]];
+      if (cudaMemcpyAsync(d_sub, hp.data(), sizeof(GenzParams) * gn, cudaMemcpyHostToDevice, s) !=
+          cudaSuccess)
+        return (int)kErrCuda;
+      detail::ParamSource<F> gs{d_sub};
+      return run_batch<kCvDim>(ws, gs, gn, per.data(), pea.data(), o, g, s);
+    }, pres, &ws);
+    if (rc != kOk && rc != kErrCapacity) return engine_status(ctx, rc);
+    for (int j = 0; j < np; ++j) result_to_c(pres[j], &out[plain_idx[j]]);
+  }
   st->ms_integrate = now_ms() - t0;
   st->mean_residual_ratio = rho_sum / count;
   return 0;
