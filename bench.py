@@ -16,8 +16,9 @@ cores with all threads, on the same workload.
 
 Under torchrun (weak scaling, no collective on the data path): for the
 single-integral workloads each rank integrates its own copy of the step's
-integrals; for batch workloads the job's world x count integrals are cut
-into contiguous shards, one per rank (cubature.parallel.shard_bounds).
+integrals; for batch workloads the job's world x count integrals are dealt
+to the ranks by a greedy split of probe costs (cubature.parallel), other
+sharded workloads cut contiguously (cubature.parallel.shard_bounds).
 Steps are bracketed by a barrier and device synchronisation, and the max
 time over ranks is used.
 """
@@ -441,6 +442,9 @@ def main() -> int:
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true",
                     help="skip timing the reference engine on the GPU beside the run")
+    ap.add_argument("--no-device-loop", action="store_true",
+                    help="long lists: the host launches every iteration (cub_options."
+                         "no_device_loop) instead of one graph launch per stretch")
     ap.add_argument("--no-cv", action="store_true",
                     help="skip the learned-control-variate side block of the default workload")
     ap.add_argument("--cv-count", type=int, default=64,
@@ -478,7 +482,7 @@ def main() -> int:
 
     # the step: integrate the workload through the public C ABI
     opts = cub.options(policy=cub.POLICY_BREADTH if workload.get("policy") == "breadth"
-                       else cub.POLICY_REFERENCE)
+                       else cub.POLICY_REFERENCE, device_loop=not args.no_device_loop)
     if "items" in workload:
         items = [cub.Integrand(f, n, a, u) for f, n, a, u in workload["items"]]
 
@@ -544,12 +548,21 @@ def main() -> int:
                                 d7["grid_z"], d7["sigma"], o) for o in offs]
     else:
         # weak scaling: `count` integrals per rank; the job's world * count
-        # integrals (seed = global index) are cut into contiguous shards
-        from cubature.parallel import shard_bounds
+        # integrals (seed = global index) are dealt to the ranks by a greedy
+        # split of their probe costs (region counts at a 100x looser
+        # tolerance, probed once before the timed steps)
+        from cubature.parallel import balanced_assignment, probe_costs
 
         fam, n, count = workload["batch"]
-        a0, b0 = shard_bounds(world * count, world, rank)
-        cases = product_peak_params(n, world * count)[a0:b0]
+        all_cases = product_peak_params(n, world * count)
+        if world > 1:
+            all_params = [cub.make_params(n, a, u) for a, u in all_cases]
+            costs = probe_costs(ctx, fam, n, all_params, workload["epsrel"], workload["epsabs"],
+                                opts)
+            mine = balanced_assignment(costs, world)[rank]
+        else:
+            mine = list(range(count))
+        cases = [all_cases[i] for i in mine]
         plist = [cub.make_params(n, a, u) for a, u in cases]
 
         def step():
@@ -765,8 +778,10 @@ def main() -> int:
                        "policy": workload.get("policy", "reference"),
                        "epsrel": workload["epsrel"], "epsabs": workload["epsabs"],
                        "parallelism": ("replicas" if "items" in workload else
-                                       f"shards{world}") if world > 1 else "single",
+                                       (f"balanced_shards{world}" if "batch" in workload
+                                        else f"shards{world}")) if world > 1 else "single",
                        "l2": "flushed between steps (256 MB write)",
+                       "device_loop": not args.no_device_loop,
                        "regions_per_step": int(sum(nreg.values())),
                        "timing": "value: CUDA events on the library's stream around each "
                                  "step's public-API calls (inputs are parameter blocks; the "

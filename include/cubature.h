@@ -121,6 +121,10 @@ typedef struct cub_options {
                               block b of the persistent kernels from
                               arriving at their grid barriers, so every
                               wait runs out; 0 = off                      */
+  int no_device_loop;      /* 1: the host launches each iteration on long
+                              lists instead of one graph launch with a
+                              conditional loop running them (same results,
+                              bit for bit)                                */
 } cub_options;
 
 /* Library version, (major << 16) | minor. */
@@ -167,6 +171,8 @@ typedef struct cub_stats {
                                     decision kernel (small batches)     */
   long long persistent_regions;  /* regions evaluated by both persistent
                                     kernels                             */
+  long long device_loops;        /* launches of the device-driven loop of
+                                    long-list iterations                */
 } cub_stats;
 
 int cub_ctx_stats(const cub_ctx* ctx, cub_stats* out);

@@ -30,6 +30,7 @@
 
 #include "engine_kernels.cuh"
 #include "persistent.cuh"
+#include "loop_graph.cuh"
 #include "phase2_kernels.cuh"
 #include "replicated.cuh"
 #include "rule9.hpp"
@@ -47,6 +48,7 @@ struct Options {
   int persistent_max_n = 0;       // list length where it hands over; 0 auto
   int persistent_max_r = 0;       // most regions per block in the persistent kernel (1,2,4,8); 0 = 8
   int replicated = 1;             // small batches: the replicated-decision kernel for short lists
+  int device_loop = 1;            // long lists: iterations driven by a conditional graph loop
   long long barrier_spins = 0;    // grid-barrier polls before a timeout; 0 = kBarrierSpins
   int hold_block = -1;            // tests: this block never arrives at a grid barrier
   // Second phase on share shard_rank of shard_world of the leftover boxes
@@ -92,6 +94,7 @@ struct Stats {
   long long persistent_launches = 0;
   long long persistent_iterations = 0;
   long long replicated_launches = 0;  // persistent launches of the replicated kernel
+  long long device_loops = 0;         // launches of the device-driven loop graph
   long long persistent_regions = 0;   // regions evaluated by both persistent kernels
 };
 
@@ -117,6 +120,7 @@ class Workspace {
   // Free every device and pinned buffer; the next run reserves afresh.
   void release() {
     drop_launch_graphs();
+    drop_loops();
     if (done_host_) cudaFreeHost(done_host_);
     done_host_ = nullptr;
     done_dev_ = nullptr;
@@ -441,6 +445,27 @@ class Workspace {
     return true;
   }
 
+  // Device-driven loops of the multi-launch iteration (loop_graph.cuh):
+  // one graph per dimension and integrand source, built on first use, with
+  // its argument block in device memory and a pinned staging copy.
+  struct LoopEntry {
+    const void* key = nullptr;  // identifies the instantiation (its bind kernel)
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    void* dargs = nullptr;  // LoopArgs<Src> on the device
+    void* hargs = nullptr;  // pinned staging copy
+  };
+  LoopEntry* find_loop(const void* key) {
+    for (auto& e : loops_)
+      if (e.key == key) return &e;
+    return nullptr;
+  }
+  LoopEntry* add_loop(const LoopEntry& e) {
+    loops_.push_back(e);
+    return &loops_.back();
+  }
+  bool loops_failed = false;  // a loop graph could not be built here: the host drives
+
   // The device control block's barrier counters are zero: set when the
   // block is cleared or uploaded and after a replicated launch (its last
   // block zeroes them), cleared after a launch of the persistent kernel.
@@ -624,6 +649,16 @@ class Workspace {
   LaunchGraph lg_[kLaunchGraphs];
   unsigned long long lg_clock_ = 0;
   bool graph_failed_ = false;
+  std::vector<LoopEntry> loops_;
+  void drop_loops() {
+    for (auto& e : loops_) {
+      if (e.exec) cudaGraphExecDestroy(e.exec);
+      if (e.graph) cudaGraphDestroy(e.graph);
+      if (e.dargs) cudaFree(e.dargs);
+      if (e.hargs) cudaFreeHost(e.hargs);
+    }
+    loops_.clear();
+  }
   static void drop_launch_graph(LaunchGraph& g) {
     if (g.exec) cudaGraphExecDestroy(g.exec);
     if (g.graph) cudaGraphDestroy(g.graph);
@@ -894,6 +929,97 @@ inline void persistent_control(Workspace& ws, const IterState& hs, int cur) {
 
 }  // namespace detail
 
+namespace detail {
+
+// The device-driven loop of dimension N and integrand source Src, built on
+// first use: WHILE { bind; SWITCH { rule with 1 | 8 | 32 lanes per region };
+// partials; decide; scan; split; advance; test }.  Grids are the largest
+// the host-driven loop uses for the lane count or step (the kernels stride
+// over the list).  Null when a graph with conditional nodes cannot be built
+// here; the host then drives the iterations.
+template <int N, class Src>
+Workspace::LoopEntry* loop_graph(Workspace& ws, int sms) {
+  const void* key = (const void*)k_loop_split<N, Src>;
+  if (Workspace::LoopEntry* found = ws.find_loop(key)) return found;
+  if (ws.loops_failed) return nullptr;
+  Workspace::LoopEntry e;
+  e.key = key;
+  cudaGraph_t g = nullptr;
+  cudaGraphConditionalHandle again = 0, lanes = 0;
+  bool ok = cudaMalloc(&e.dargs, sizeof(LoopArgs<Src>)) == cudaSuccess &&
+            cudaHostAlloc(&e.hargs, sizeof(LoopArgs<Src>), cudaHostAllocDefault) == cudaSuccess &&
+            cudaGraphCreate(&g, 0) == cudaSuccess &&
+            cudaGraphConditionalHandleCreate(&again, g, 1, cudaGraphCondAssignDefault) ==
+                cudaSuccess &&
+            cudaGraphConditionalHandleCreate(&lanes, g, 0, 0) == cudaSuccess;
+  cudaGraph_t body = nullptr;
+  if (ok) {
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = again;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t wn;
+    ok = cudaGraphAddNode(&wn, g, nullptr, 0, &cp) == cudaSuccess;
+    if (ok) body = cp.conditional.phGraph_out[0];
+  }
+  auto kernel = [&](cudaGraph_t gr, cudaGraphNode_t* dep, const void* fn, int grid, int block,
+                    void** args, cudaGraphNode_t* out) {
+    cudaKernelNodeParams kp = {};
+    kp.func = const_cast<void*>(fn);
+    kp.gridDim = dim3((unsigned)grid);
+    kp.blockDim = dim3((unsigned)block);
+    kp.sharedMemBytes = 0;
+    kp.kernelParams = args;
+    kp.extra = nullptr;
+    return cudaGraphAddKernelNode(out, gr, dep, dep ? 1 : 0, &kp) == cudaSuccess;
+  };
+  LoopArgs<Src>* la = static_cast<LoopArgs<Src>*>(e.dargs);
+  const LoopArgs<Src>* lac = la;
+  void* a_bind[] = {(void*)&la, (void*)&lanes};
+  void* a_la[] = {(void*)&lac};
+  const RuleTables T = make_rule9_tables(N);
+  void* a_eval[] = {(void*)&lac, (void*)&T};
+  void* a_test[] = {(void*)&lac, (void*)&again};
+  cudaGraphNode_t n_bind = nullptr, n_sw = nullptr, n_part = nullptr, n_dec = nullptr,
+                  n_scan = nullptr, n_split = nullptr, n_adv = nullptr, n_test = nullptr, n_ev;
+  ok = ok && kernel(body, nullptr, (const void*)k_loop_bind<Src>, 1, 32, a_bind, &n_bind);
+  cudaGraph_t arms[3] = {nullptr, nullptr, nullptr};
+  if (ok) {
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = lanes;
+    cp.conditional.type = cudaGraphCondTypeSwitch;
+    cp.conditional.size = 3;
+    ok = cudaGraphAddNode(&n_sw, body, &n_bind, 1, &cp) == cudaSuccess;
+    if (ok)
+      for (int i = 0; i < 3; ++i) arms[i] = cp.conditional.phGraph_out[i];
+  }
+  ok = ok && kernel(arms[0], nullptr, (const void*)k_loop_eval<N, 1, Src>, sms * 32, 256, a_eval, &n_ev);
+  ok = ok && kernel(arms[1], nullptr, (const void*)k_loop_eval<N, 8, Src>, sms * 16, 256, a_eval, &n_ev);
+  ok = ok && kernel(arms[2], nullptr, (const void*)k_loop_eval<N, 32, Src>, sms * 8, 256, a_eval, &n_ev);
+  ok = ok && kernel(body, &n_sw, (const void*)k_loop_partials<Src>, sms * 16, 256, a_la, &n_part);
+  ok = ok && kernel(body, &n_part, (const void*)k_loop_decide<Src>, sms * 16, 256, a_la, &n_dec);
+  ok = ok && kernel(body, &n_dec, (const void*)k_loop_scan<Src>, 1, 32, a_la, &n_scan);
+  ok = ok && kernel(body, &n_scan, (const void*)k_loop_split<N, Src>, sms * 16, 256, a_la, &n_split);
+  ok = ok && kernel(body, &n_split, (const void*)k_loop_advance<Src>, sms, 256, a_la, &n_adv);
+  ok = ok && kernel(body, &n_adv, (const void*)k_loop_test<Src>, 1, 32, a_test, &n_test);
+  ok = ok && cudaGraphInstantiate(&e.exec, g, 0) == cudaSuccess;
+  if (!ok) {
+    if (e.exec) cudaGraphExecDestroy(e.exec);
+    if (g) cudaGraphDestroy(g);
+    if (e.dargs) cudaFree(e.dargs);
+    if (e.hargs) cudaFreeHost(e.hargs);
+    ws.loops_failed = true;
+    cudaGetLastError();
+    return nullptr;
+  }
+  e.graph = g;
+  return ws.add_loop(e);
+}
+
+}  // namespace detail
+
 // Rule evaluation step of the multi-launch driver when the caller supplies
 // its own (NoHook: the engine's k_eval).  A hook's eval(args, n, stream)
 // evaluates the n slots of the current list into args.avg/err/axis/active
@@ -1119,6 +1245,59 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
       st.launches += 1;
       grid_pending = false;
     }
+    // Device-driven iterations (loop_graph.cuh): one graph launch runs them
+    // until the list needs larger buffers, goes back to a persistent
+    // kernel's range or no integral is running.  Timing keeps the
+    // host-driven loop, which records events around each rule launch.
+    Workspace::LoopEntry* loop = nullptr;
+    if constexpr (!Hook::kActive) {
+      if (opt.device_loop && !ws.timing) loop = detail::loop_graph<N, Src>(ws, sms);
+    }
+    if (loop) {
+      LoopArgs<Src>& la = *static_cast<LoopArgs<Src>*>(loop->hargs);
+      std::memset(&la, 0, sizeof(la));
+      for (int b = 0; b < 2; ++b) {
+        EngineArgs ab = a;
+        detail::bind_lists(ws, ab, b, 0);
+        la.base[b] = ab;
+      }
+      la.src = src;
+      // the host's own limit too: the buffers may be larger than max_slots
+      // (grown by an earlier call), and a list beyond it stops the run
+      la.cap = std::min<long long>(ws.cap(), max_slots);
+      la.left_cap = ws.left_cap();
+      la.ref_policy = opt.policy == kPolicyReference ? 1 : 0;
+      const int hb_p = pblocks > 0 ? pmax : 0;
+      const int hb_r = rblocks > 0 ? rmax : 0;
+      la.hand_back = std::max(hb_p, hb_r);
+      la.k1_min = sms * 512;
+      la.k8_min = sms * 64;
+      la.forced_lanes = opt.lanes > 0 ? opt.lanes : 0;
+      if (!ws.ck(cudaMemcpyAsync(loop->dargs, loop->hargs, sizeof(la), cudaMemcpyHostToDevice, s)) ||
+          !ws.ck(cudaGraphLaunch(loop->exec, s)) ||
+          !ws.ck(cudaMemcpyAsync(loop->hargs, loop->dargs, sizeof(la), cudaMemcpyDeviceToHost, s)) ||
+          !ws.ck(cudaMemcpyAsync(ws.ctl_host_, ws.ctl, sizeof(Control), cudaMemcpyDeviceToHost, s)) ||
+          !ws.ck(cudaStreamSynchronize(s)))
+        return kErrCuda;
+      st.h2d_bytes += (long long)sizeof(la);
+      st.d2h_bytes += (long long)(sizeof(la) + sizeof(Control));
+      st.iterations += la.iterations;
+      st.eval_launches += la.iterations;
+      st.regions_evaluated += (long long)la.regions;
+      st.launches += 7ll * la.iterations;
+      st.device_loops += 1;
+      ws.peak_need = std::max(ws.peak_need, la.peak_need);
+      c0.iters_done = ws.ctl_host_->iters_done;
+      const IterState nx = ws.ctl_host_->host;
+      if (nx.overflow) {
+        status = kErrCapacity;
+        break;
+      }
+      cur = ws.ctl_host_->cur;
+      hs = nx;
+      n_left = nx.n_left;
+      continue;
+    }
     int K = opt.lanes;
     if (K <= 0) K = n_cur >= (long long)sms * 512 ? 1 : (n_cur >= (long long)sms * 64 ? 8 : 32);
     if (ws.timing) ws.ck(cudaEventRecord(ws.ev[0], s));
@@ -1204,15 +1383,27 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
   if (status == kOk && n_left > 0) {
     // phase 2 on the leftover boxes [box0, box1)
     states_fresh = false;
+    // the heaps in shared memory when two blocks of them fit on an SM (the
+    // default 2048 bisections: 98 KB a block), else in the global slab
+    const size_t heap_smem = detail::phase2_heap_smem(opt.phase2_max_regions);
+    const bool smem_heap =
+        heap_smem <= 100 * 1024 &&
+        cudaFuncSetAttribute(k_phase2<N, Src, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)heap_smem) == cudaSuccess;
+    if (!smem_heap) cudaGetLastError();
     int dev_blocks = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&dev_blocks, k_phase2<N, Src>, 128, 0);
+    if (smem_heap)
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&dev_blocks, k_phase2<N, Src, true>, 128,
+                                                    heap_smem);
+    else
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&dev_blocks, k_phase2<N, Src, false>, 128, 0);
     dev_blocks = std::max(1, dev_blocks);
     long long blocks = std::min<long long>((long long)sms * dev_blocks, (box1 - box0 + 3) / 4);
     blocks = std::max<long long>(blocks, 1);
     const long long nwarps = blocks * 4;
     const int stride = opt.phase2_max_regions + 2;
     if (!ws.reserve_slab(sizeof(P2Region<N>) * nwarps * stride,
-                         (size_t)nwarps * stride * (sizeof(P2HeapEnt) / sizeof(int))))
+                         smem_heap ? 1 : (size_t)nwarps * stride * (sizeof(P2HeapEnt) / sizeof(int))))
       return kErrCuda;
     if (shard) {
       // boxes of other shares contribute nothing to the collection
@@ -1240,7 +1431,10 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
     // one integral's shares follow the reference's leftover order
     p.pair_half = shard && opt.shard_world > 1 && nint == 1 ? (int)(n_left / 2) : 0;
     if (ws.timing) ws.ck(cudaEventRecord(ws.ev[2], s));
-    k_phase2<N, Src><<<(unsigned)blocks, 128, 0, s>>>(src, T, p);
+    if (smem_heap)
+      k_phase2<N, Src, true><<<(unsigned)blocks, 128, heap_smem, s>>>(src, T, p);
+    else
+      k_phase2<N, Src, false><<<(unsigned)blocks, 128, 0, s>>>(src, T, p);
     if (ws.timing) ws.ck(cudaEventRecord(ws.ev[3], s));
     st.phase2_boxes += box1 - box0;
     const unsigned cb = (unsigned)std::max(1, std::min((nint + 7) / 8, sms * 16));
@@ -1283,6 +1477,11 @@ struct Replay {
   int per = 0, padded = 0;
   long long n0 = 0;
   PersistArgs p;
+  // batches of up to kSmallBatch integrals whose initial grid is within the
+  // replicated kernel's range launch it instead, as run_batch does
+  bool rep = false;
+  int rblocks = 0;
+  RepArgs rp;
 };
 
 template <int N, class Src>
@@ -1326,6 +1525,17 @@ int replay_prepare(Workspace& ws, int nint, const Options& opt, cudaStream_t s, 
   r->p = detail::persist_args(ws, a, opt, 0, pmax, true, dv, per, padded, nullptr);
   r->p.host_out = ws.direct_states(nint);
   r->p.host_words = (int)(ws.state_bytes(nint) / 8);
+  const int rblocks = opt.persistent && opt.replicated && nint <= kSmallBatch
+                          ? detail::replicated_blocks<N, Src>(ws, sms)
+                          : 0;
+  const int rmax = detail::replicated_limit(opt, rblocks);
+  r->rep = rblocks > 0 && n0 <= rmax;
+  if (r->rep) {
+    r->rblocks = rblocks;
+    r->rp = detail::rep_args(ws, a, opt, 0, rmax, true, dv, per, padded, nullptr);
+    r->rp.host_out = ws.direct_states(nint);
+    r->rp.host_words = (int)(ws.state_bytes(nint) / 8);
+  }
   return kOk;
 }
 
@@ -1350,13 +1560,17 @@ int replay_enqueue(Workspace& ws, const Src& src, const Replay& r, cudaStream_t 
   attr[0].id = cudaLaunchAttributeCooperative;
   attr[0].val.cooperative = 1;
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3((unsigned)r.pblocks);
+  cfg.gridDim = dim3((unsigned)(r.rep ? r.rblocks : r.pblocks));
   cfg.blockDim = dim3(256);
   cfg.dynamicSmemBytes = 0;
   cfg.stream = s;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  if (!ws.ck(cudaLaunchKernelEx(&cfg, k_persistent<N, Src>, src, T, r.p))) return kErrCuda;
+  if (r.rep) {
+    if (!ws.ck(cudaLaunchKernelEx(&cfg, k_replicated<N, Src>, src, T, r.rp))) return kErrCuda;
+  } else if (!ws.ck(cudaLaunchKernelEx(&cfg, k_persistent<N, Src>, src, T, r.p))) {
+    return kErrCuda;
+  }
   if (!r.p.host_out &&
       !ws.ck(cudaMemcpyAsync(ws.ctl_host_, ws.ctl, bytes, cudaMemcpyDeviceToHost, s)))
     return kErrCuda;

@@ -103,6 +103,79 @@ __device__ __forceinline__ int heap_pop(P2HeapEnt* heap, int& hn) {
   return top;
 }
 
+// The same heap with keys and indices in separate arrays (shared memory:
+// 12 bytes an entry).  Same comparisons in the same order as heap_push /
+// heap_pop, so the same bisection order.
+__device__ __forceinline__ void heap_push_soa(double* key, int* id, int& hn, int idx, double err) {
+  int i = hn++;
+  while (i > 0) {
+    const int p = (i - 1) / 2;
+    const double pk = key[p];
+    if (pk >= err) break;
+    key[i] = pk;
+    id[i] = id[p];
+    i = p;
+  }
+  key[i] = err;
+  id[i] = idx;
+}
+
+__device__ __forceinline__ int heap_pop_soa(double* key, int* id, int& hn) {
+  const int top = id[0];
+  --hn;
+  const double ek = key[hn];
+  const int ei = id[hn];
+  int i = 0;
+  for (;;) {
+    const int l = 2 * i + 1, r = l + 1;
+    int m = i;
+    double km = ek;
+    if (l < hn) {
+      const double kl = key[l];
+      if (kl > km) {
+        m = l;
+        km = kl;
+      }
+    }
+    if (r < hn && key[r] > km) m = r;
+    if (m == i) break;
+    key[i] = key[m];
+    id[i] = id[m];
+    i = m;
+  }
+  key[i] = ek;
+  id[i] = ei;
+  return top;
+}
+
+// A warp's heap: in the global slab (kShared = false) or in the block's
+// dynamic shared memory (keys of the block's four warps, then their
+// indices).
+template <bool kShared>
+struct P2Heap;
+
+template <>
+struct P2Heap<false> {
+  P2HeapEnt* h;
+  __device__ __forceinline__ void push(int& hn, int idx, double err) { heap_push(h, hn, idx, err); }
+  __device__ __forceinline__ int pop(int& hn) { return heap_pop(h, hn); }
+};
+
+template <>
+struct P2Heap<true> {
+  double* key;
+  int* id;
+  __device__ __forceinline__ void push(int& hn, int idx, double err) {
+    heap_push_soa(key, id, hn, idx, err);
+  }
+  __device__ __forceinline__ int pop(int& hn) { return heap_pop_soa(key, id, hn); }
+};
+
+// Dynamic shared memory of one block of the shared-heap phase-2 kernel.
+inline size_t phase2_heap_smem(int max_regions) {
+  return (size_t)4 * (size_t)(max_regions + 2) * (sizeof(double) + sizeof(int));
+}
+
 // Evaluate subregion `reg` of box (BL, BW) with the 16 lanes of a half warp.
 template <int N, class F>
 __device__ __forceinline__ RegionResult eval_sub(const F& f, const double (&BL)[N],
@@ -133,12 +206,18 @@ __device__ __forceinline__ RegionResult eval_sub(const F& f, const double (&BL)[
 
 }  // namespace detail
 
-// Three blocks (12 warps) per SM: each warp refines its box serially, so
-// warps in flight hide the latency of the heap and the rule; the register
-// cap this sets costs a few spilled words.
-template <int N, class Src>
-__global__ void __launch_bounds__(128, 3) k_phase2(Src src, RuleTables T, Phase2Args a) {
+// kShared = false: three blocks (12 warps) per SM, each warp's heap in the
+// global slab -- each warp refines its box serially, so warps in flight
+// hide the latency of the heap and the rule; the register cap this sets
+// costs a few spilled words.  kShared = true: the heaps in shared memory
+// (phase2_heap_smem bytes a block, two blocks per SM at the default 2048
+// bisections), so a heap level costs a shared-memory access instead of an
+// L2 round trip.
+template <int N, class Src, bool kShared = false>
+__global__ void __launch_bounds__(128, kShared ? 2 : 3) k_phase2(Src src, RuleTables T,
+                                                                 Phase2Args a) {
   __shared__ detail::ItemTable<N> tab;
+  extern __shared__ double p2_dyn[];
   if (threadIdx.x == 0) tab.fill();
   __syncthreads();
 
@@ -148,7 +227,14 @@ __global__ void __launch_bounds__(128, 3) k_phase2(Src src, RuleTables T, Phase2
   const long long gwarp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / 32;
   const int stride = a.max_regions + 2;
   P2Region<N>* pool = reinterpret_cast<P2Region<N>*>(a.slab) + gwarp * stride;
-  P2HeapEnt* heap = a.heap + gwarp * stride;
+  detail::P2Heap<kShared> heap;
+  if constexpr (kShared) {
+    const int w = threadIdx.x >> 5;
+    heap.key = p2_dyn + (size_t)w * stride;
+    heap.id = reinterpret_cast<int*>(p2_dyn + (size_t)4 * stride) + (size_t)w * stride;
+  } else {
+    heap.h = a.heap + gwarp * stride;
+  }
 
   for (;;) {
     int box = 0;
@@ -183,7 +269,7 @@ __global__ void __launch_bounds__(128, 3) k_phase2(Src src, RuleTables T, Phase2
     double ERR = r0.err, RESULT = r0.avg;
     if (lane == 0) {
       pool[0] = r0;
-      detail::heap_push(heap, hn, 0, r0.err);
+      heap.push(hn, 0, r0.err);
     }
     __syncwarp();
     int nreg = 1;
@@ -191,7 +277,7 @@ __global__ void __launch_bounds__(128, 3) k_phase2(Src src, RuleTables T, Phase2
            (nreg == 1 || ERR > detail::max_err(RESULT, epsrel, epsabs));
          ++nreg) {
       int pi = 0;
-      if (lane == 0) pi = detail::heap_pop(heap, hn);
+      if (lane == 0) pi = heap.pop(hn);
       pi = __shfl_sync(0xffffffffu, pi, 0);
       __syncwarp();
       const P2Region<N> parent = pool[pi];
@@ -241,8 +327,8 @@ __global__ void __launch_bounds__(128, 3) k_phase2(Src src, RuleTables T, Phase2
         right.axis = axR;
         pool[pi] = left;
         pool[used] = right;
-        detail::heap_push(heap, hn, pi, errL);
-        detail::heap_push(heap, hn, used, errR);
+        heap.push(hn, pi, errL);
+        heap.push(hn, used, errR);
       }
       ++used;
       ERR = __shfl_sync(0xffffffffu, ERR, 0);

@@ -70,6 +70,7 @@ Options to_options(const cub_options* opt) {
   o.replicated = opt->no_replicated ? 0 : 1;
   if (opt->barrier_spins > 0) o.barrier_spins = opt->barrier_spins;
   o.hold_block = opt->test_hold_block > 0 ? opt->test_hold_block - 1 : -1;
+  o.device_loop = opt->no_device_loop ? 0 : 1;
   return o;
 }
 
@@ -152,6 +153,7 @@ void cub_default_options(cub_options* opt) {
   opt->no_replicated = o.replicated ? 0 : 1;
   opt->barrier_spins = 0;
   opt->test_hold_block = 0;
+  opt->no_device_loop = o.device_loop ? 0 : 1;
 }
 
 cub_ctx* cub_create(int device) {
@@ -216,6 +218,7 @@ int cub_ctx_stats(const cub_ctx* ctx, cub_stats* out) {
   out->persistent_iterations = s.persistent_iterations;
   out->replicated_launches = s.replicated_launches;
   out->persistent_regions = s.persistent_regions;
+  out->device_loops = s.device_loops;
   return 0;
 }
 

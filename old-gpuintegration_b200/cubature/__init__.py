@@ -83,6 +83,7 @@ class CStats(C.Structure):
         ("persistent_iterations", C.c_longlong),
         ("replicated_launches", C.c_longlong),
         ("persistent_regions", C.c_longlong),
+        ("device_loops", C.c_longlong),
     ]
 
     def as_dict(self) -> dict:
@@ -103,6 +104,7 @@ class COptions(C.Structure):
         ("no_replicated", C.c_int),
         ("barrier_spins", C.c_longlong),
         ("test_hold_block", C.c_int),
+        ("no_device_loop", C.c_int),
     ]
 
 
@@ -319,7 +321,7 @@ def options(policy: int = POLICY_REFERENCE, phase1_cap: int = 0, max_iters: int 
             phase2_max_regions: int = 0, max_slots: int = 0, lanes: int = 0,
             persistent: bool = True, persistent_max_n: int = 0,
             persistent_max_r: int = 0, replicated: bool = True, barrier_spins: int = 0,
-            test_hold_block: int = -1) -> COptions:
+            test_hold_block: int = -1, device_loop: bool = True) -> COptions:
     o = COptions()
     load_library().cub_default_options(C.byref(o))
     o.policy = policy
@@ -340,6 +342,7 @@ def options(policy: int = POLICY_REFERENCE, phase1_cap: int = 0, max_iters: int 
     o.no_replicated = 0 if replicated else 1
     o.barrier_spins = barrier_spins
     o.test_hold_block = test_hold_block + 1 if test_hold_block >= 0 else 0
+    o.no_device_loop = 0 if device_loop else 1
     return o
 
 

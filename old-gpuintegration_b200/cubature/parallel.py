@@ -5,6 +5,11 @@ between GPUs, gloo on CPU).
   into contiguous shards, one per rank, and each rank integrates its shard
   on its own device with no communication on the data path.  One gather of
   fixed-size result records at the end gives every rank the full list.
+* Batches of uneven difficulty (integrate_balanced,
+  integrate_batch_balanced): the integrals are dealt to the ranks by a
+  greedy longest-first split of estimated costs -- the region counts of a
+  cheap probe at a looser tolerance, each rank probing a contiguous shard
+  and one gather sharing the counts -- so that the ranks finish together.
 * One integral (integrate_split): the reference's own multi-device split
   (GPUquad.h:430-609, GPUKernelquad.cu:729-906).  Every rank runs the same
   breadth-first first phase (deterministic, so the ranks agree on the
@@ -92,6 +97,94 @@ def integrate_sharded(integrate: Callable[[int, int], Sequence[Result]], count: 
         host = parts[r].cpu()
         out.extend(_unpack(host[i]) for i in range(b - a))
     return out
+
+
+def balanced_assignment(costs: Sequence[float], world: int) -> list[list[int]]:
+    """Greedy longest-first split of items with the given costs over `world`
+    ranks: items in decreasing cost (ties by index) each go to the rank with
+    the least total so far (ties to the lowest rank).  Each rank's indices
+    come back in increasing order.  Deterministic, so every rank computes
+    the same split from the same costs."""
+    if world <= 0:
+        raise ValueError("bad world size")
+    load = [0.0] * world
+    out: list[list[int]] = [[] for _ in range(world)]
+    for i in sorted(range(len(costs)), key=lambda j: (-float(costs[j]), j)):
+        r = min(range(world), key=lambda q: (load[q], q))
+        out[r].append(i)
+        load[r] += float(costs[i])
+    for lst in out:
+        lst.sort()
+    return out
+
+
+def _gather_rows(local: Sequence[Result], rows: int, failed: bool, message: str, world: int,
+                 group):
+    device = torch.device("cuda", torch.cuda.current_device()) \
+        if dist.get_backend(group) == "nccl" else torch.device("cpu")
+    mine = _pack(local, rows, failed, device)
+    parts = [torch.empty_like(mine) for _ in range(world)]
+    dist.all_gather(parts, mine, group=group)
+    bad = [r for r in range(world) if float(parts[r][0, -1]) != 0.0]
+    if bad:
+        raise CubatureError(ERR_INVALID, message or f"integration failed on rank(s) {bad}")
+    return [p.cpu() for p in parts]
+
+
+def integrate_balanced(integrate: Callable[[list[int]], Sequence[Result]],
+                       costs: Sequence[float], group=None) -> list[Result]:
+    """Run integrate(indices) on this rank's share of the batch, the share
+    chosen by balanced_assignment(costs, world), and return the results of
+    all ranks in batch order on every rank (one gather).  Without an
+    initialised process group this is a plain call on every index."""
+    count = len(costs)
+    if not (dist.is_available() and dist.is_initialized()):
+        return list(integrate(list(range(count))))
+    world = dist.get_world_size(group)
+    rank = dist.get_rank(group)
+    shares = balanced_assignment(costs, world)
+    rows = max(1, max(len(sh) for sh in shares))
+    failed, message = False, ""
+    try:
+        local = list(integrate(shares[rank])) if shares[rank] else []
+        if len(local) != len(shares[rank]):
+            raise CubatureError(ERR_INVALID, "share returned the wrong number of results")
+    except Exception as exc:  # every rank must still reach the gather
+        failed, message, local = True, f"rank {rank}: {exc}", []
+    parts = _gather_rows(local, rows, failed, message, world, group)
+    out: list[Result | None] = [None] * count
+    for r in range(world):
+        for i, idx in enumerate(shares[r]):
+            out[idx] = _unpack(parts[r][i])
+    return out  # type: ignore[return-value]
+
+
+def probe_costs(ctx, family, ndim: int, params: Sequence, epsrel: float, epsabs: float,
+                opts=None, factor: float = 100.0, group=None) -> list[float]:
+    """Estimated cost of each integral of a batch: its region count at
+    epsrel * factor (a run a small fraction of the real one's cost).  Each
+    rank probes a contiguous shard; one gather gives every rank all counts."""
+    loose = min(0.5, epsrel * factor)
+
+    def run(a: int, b: int):
+        return ctx.integrate_batch(family, ndim, list(params)[a:b], loose, epsabs, opts)
+
+    return [float(r.nregions) for r in integrate_sharded(run, len(params), group)]
+
+
+def integrate_batch_balanced(ctx, family, ndim: int, params: Sequence, epsrel, epsabs,
+                             opts=None, group=None, costs: Sequence[float] | None = None
+                             ) -> list[Result]:
+    """ctx.integrate_batch over all ranks with a difficulty-balanced split
+    (probe_costs when no costs are given); scalar tolerances."""
+    if costs is None:
+        costs = probe_costs(ctx, family, ndim, params, epsrel, epsabs, opts, group=group)
+    plist = list(params)
+
+    def run(idx: list[int]):
+        return ctx.integrate_batch(family, ndim, [plist[i] for i in idx], epsrel, epsabs, opts)
+
+    return integrate_balanced(run, costs, group)
 
 
 _NONFINITE = 1 << 30

@@ -835,3 +835,34 @@ def test_split_second_phase_matches_whole_integral(cub, oracle, ctx, world):
         res = P.integrate_split(lambda r, w: ctx.integrate_shard(f, 1e-7, 1e-12, r, w, opts),
                                 1e-7, 1e-12)
         assert res.nregions == whole.nregions and res.status == whole.status
+
+
+def test_device_loop_bit_identical(cub, ctx):
+    """Long lists run their iterations as one graph launch with a
+    conditional loop (bind, rule, partials, decide, scan, split, advance,
+    test) instead of host-launched chains: the same kernels in the same
+    order, so results are identical bit for bit -- a batch of 64 6-D
+    product peaks whose lists outgrow the persistent kernel (breadth policy
+    and the reference policy with phase-2 hand-over), a single 8-D corner
+    peak under a small persistent limit, and a breadth batch under a small
+    capacity whose loop leaves to grow the buffers."""
+    rng = np.random.default_rng(21)
+    n = 6
+    params = [cub.make_params(n, list(np.exp(rng.uniform(0, np.log(50), n))),
+                              list(rng.uniform(0.1, 0.9, n))) for _ in range(64)]
+    for opts in ({"policy": cub.POLICY_BREADTH}, {"phase1_cap": 8192},
+                 {"policy": cub.POLICY_BREADTH, "max_slots": 1 << 18}):
+        ctx.reset_stats()
+        r1 = ctx.integrate_batch("product_peak", n, params, 1e-5, 1e-12, cub.options(**opts))
+        loops = ctx.stats()["device_loops"]
+        r2 = ctx.integrate_batch("product_peak", n, params, 1e-5, 1e-12,
+                                 cub.options(device_loop=False, **opts))
+        assert loops > 0, opts
+        for k, (x, y) in enumerate(zip(r1, r2)):
+            _same_bits(x, y, (opts, k))
+    f = cub.Integrand("corner_peak", 8, 0.5, 0.0)
+    ctx.reset_stats()
+    r1 = ctx.integrate(f, 1e-7, 1e-12, cub.options(persistent_max_n=64))
+    assert ctx.stats()["device_loops"] > 0
+    r2 = ctx.integrate(f, 1e-7, 1e-12, cub.options(persistent_max_n=64, device_loop=False))
+    _same_bits(r1, r2, "corner peak")

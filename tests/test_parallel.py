@@ -110,13 +110,30 @@ def _worker(rank, world, port, count, fail_rank, q, mode="batch"):
                 raise RuntimeError("injected failure")
             return _oracle_shard(cases, a, b)
 
+        def share(idx):
+            if rank == fail_rank:
+                raise RuntimeError("injected failure")
+            return [_oracle_shard(cases, i, i + 1)[0] for i in idx]
+
         try:
-            res = P.integrate_sharded(shard, count)
+            if mode == "balanced":
+                # costs: the integrals' region counts at a 100x looser tolerance
+                res = P.integrate_balanced(share, _probe_costs(cases))
+            else:
+                res = P.integrate_sharded(shard, count)
             q.put((rank, "ok", [(r.integral, r.nregions, r.status) for r in res]))
         except P.CubatureError as exc:
             q.put((rank, "error", str(exc)))
     finally:
         dist.destroy_process_group()
+
+
+def _probe_costs(cases):
+    import oracle as O
+
+    R = O.Rule(3)
+    return [float(R.integrate_reference(O.make_integrand("product_peak", 3, av, uv), 1e-4,
+                                        1e-12)["nregions"]) for av, uv in cases]
 
 
 def _free_port():
@@ -197,3 +214,44 @@ def test_split_world_one_is_the_plain_result():
     assert (res.nregions, res.neval, res.status) == (ref["nregions"], ref["neval"],
                                                      ref["status"])
     assert res.integral == ref["value"] and res.error == ref["error"]
+
+
+def test_balanced_assignment_covers_and_balances():
+    """The greedy longest-first split deals every item to exactly one rank,
+    is the same on every call, keeps each rank's items in batch order, and
+    stays within one item's cost of the best balance (the greedy bound);
+    on skewed costs it balances far better than contiguous shards."""
+    import numpy as np
+
+    rng = np.random.default_rng(3)
+    for count, world in [(0, 2), (1, 3), (7, 2), (100, 3), (4096, 8)]:
+        costs = list(np.exp(rng.uniform(0, 6, count)))
+        sh = P.balanced_assignment(costs, world)
+        assert sh == P.balanced_assignment(costs, world)
+        flat = sorted(i for s_ in sh for i in s_)
+        assert flat == list(range(count))
+        assert all(s_ == sorted(s_) for s_ in sh)
+        if count:
+            loads = [sum(costs[i] for i in s_) for s_ in sh]
+            assert max(loads) - min(loads) <= max(costs) + 1e-9
+    costs = [100.0] * 4 + [1.0] * 60  # the hard integrals first, as in a sorted batch
+    loads_b = [sum(costs[i] for i in s_) for s_ in P.balanced_assignment(costs, 4)]
+    loads_c = [sum(costs[a:b]) for a, b in (P.shard_bounds(64, 4, r) for r in range(4))]
+    assert max(loads_b) < 0.5 * max(loads_c)
+    with pytest.raises(ValueError):
+        P.balanced_assignment([1.0], 0)
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_balanced_matches_serial(world):
+    """Ranks integrating difficulty-balanced shares (probe costs at a looser
+    tolerance) return the whole batch, in batch order, identical to one
+    process; a failure on one rank reaches every rank."""
+    count = 9
+    serial = [(r.integral, r.nregions, r.status) for r in _oracle_shard(_cases(count), 0, count)]
+    out = _run(world, count, mode="balanced")
+    assert [o[1] for o in out] == ["ok"] * world
+    for _, _, res in out:
+        assert res == serial
+    out = _run(world, count, fail_rank=world - 1, mode="balanced")
+    assert [o[1] for o in out] == ["error"] * world
