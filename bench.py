@@ -445,6 +445,9 @@ def main() -> int:
     ap.add_argument("--no-device-loop", action="store_true",
                     help="long lists: the host launches every iteration (cub_options."
                          "no_device_loop) instead of one graph launch per stretch")
+    ap.add_argument("--no-check-exit", action="store_true",
+                    help="exit 0 even when integrals miss the check (profiling runs of "
+                         "workloads whose misses are the algorithm's own)")
     ap.add_argument("--no-cv", action="store_true",
                     help="skip the learned-control-variate side block of the default workload")
     ap.add_argument("--cv-count", type=int, default=64,
@@ -834,7 +837,7 @@ def main() -> int:
         pg.destroy_process_group()
     # integrals that miss the analytic value by more than 2 epsrel (or do not
     # converge) are counted in "check" and fail the run
-    return 1 if bad else 0
+    return 1 if bad and not args.no_check_exit else 0
 
 
 if __name__ == "__main__":
