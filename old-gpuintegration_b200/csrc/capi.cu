@@ -280,6 +280,40 @@ int integrate_impl(cub_ctx* ctx, int family, int ndim, int count, const cub_genz
   if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
   static_assert(sizeof(cub_genz_params) == sizeof(GenzParams), "params layout");
   const GenzParams* h = reinterpret_cast<const GenzParams*>(params);
+  if (count == 1) {
+    // one integral (the drop-in call): no grouping and no staging vectors;
+    // the same run as a group of one
+    const double er1 = epsrel ? epsrel[0] : epsrel0, ea1 = epsabs ? epsabs[0] : epsabs0;
+    if (!(er1 >= 0) || !(ea1 >= 0)) {
+      set_error("epsrel/epsabs must be >= 0");
+      return CUB_ERR_INVALID;
+    }
+    Options o = to_options(opt);
+    if (o.max_slots <= 0) o.max_slots = ctx->ws->auto_slots(ndim, o.policy);
+    o.shard_rank = ctx->shard_rank;
+    o.shard_world = ctx->shard_world;
+    double box[2 * kMaxDim];
+    if (lo)
+      for (int d = 0; d < ndim; ++d) {
+        box[d] = lo[d];
+        box[ndim + d] = hi[d];
+      }
+    Result r{};
+    const int rc = dispatch_run(ctx, family, ndim, 1, h, nullptr, &er1, &ea1, o, &r,
+                                lo ? box : nullptr);
+    if (rc == kErrCuda) {
+      set_error(ctx->ws->error());
+      return CUB_ERR_CUDA;
+    }
+    if (rc == kErrTimeout) {
+      set_error("a device-side grid barrier wait ran out (persistent kernel)");
+      return CUB_ERR_TIMEOUT;
+    }
+    if (rc == kErrCapacity) set_error("region capacity exceeded; results are the last estimates");
+    if (rc < 0 && rc != kErrCapacity) return rc;
+    to_c(r, out);
+    return rc == kErrCapacity ? CUB_ERR_CAPACITY : 0;
+  }
   std::vector<double> er(count), ea(count);
   for (int k = 0; k < count; ++k) {
     er[k] = epsrel ? epsrel[k] : epsrel0;
