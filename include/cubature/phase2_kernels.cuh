@@ -9,13 +9,17 @@
 // boxes from an atomic counter.  Each step bisects the box's exact maximum
 // error subregion (a binary heap kept by lane 0, each entry holding the
 // subregion's error beside its index), and the two children are
-// evaluated in parallel by the two 16-lane halves of the warp.  Subregions
+// evaluated in parallel by the two 16-lane halves of the warp: rule point
+// p on lane p % 16, in rounds whose generator sets are fixed at compile
+// time (the replicated kernel's coefficient-code table and round plan), so
+// the 16 lanes carry the same number of points.  Subregions
 // live in a per-warp slab of global memory preallocated by the host, so
 // there is no device malloc and the footprint is fixed by the grid size.
 // Every loop is bounded (at most max_regions steps per box).
 #pragma once
 
 #include "engine_kernels.cuh"
+#include "replicated.cuh"
 
 namespace cubature {
 
@@ -176,12 +180,18 @@ inline size_t phase2_heap_smem(int max_regions) {
   return (size_t)4 * (size_t)(max_regions + 2) * (sizeof(double) + sizeof(int));
 }
 
-// Evaluate subregion `reg` of box (BL, BW) with the 16 lanes of a half warp.
+// Evaluate subregion `reg` of box (BL, BW) with the 16 lanes of a half
+// warp, table-driven: round r holds points 16 r .. 16 r + 15 (Rounds<N,
+// 16>), the lanes' set sums are combined by shuffles within the half, and
+// the fourth difference comes from the staged centre and set-1/2 values
+// (fst, one staging row per half warp).  Every lane of the half returns
+// the result.
 template <int N, class F>
-__device__ __forceinline__ RegionResult eval_sub(const F& f, const double (&BL)[N],
-                                                 const double (&BW)[N], const P2Region<N>& reg,
-                                                 int hlane, unsigned hmask, const ItemTable<N>& tab,
-                                                 const RuleTables& T) {
+__device__ __forceinline__ RegionResult eval_sub_tab(const F& f, const double (&BL)[N],
+                                                     const double (&BW)[N], const P2Region<N>& reg,
+                                                     int hlane, unsigned hmask,
+                                                     const ByteTable<N>& tb, double* fst,
+                                                     const RuleTables& T) {
   double L[N], H[N];
   int widest = 0;
   double wmax = 0;
@@ -196,8 +206,38 @@ __device__ __forceinline__ RegionResult eval_sub(const F& f, const double (&BL)[
     }
   }
   RegionSums rs;
-  region_point_sums<N, 16>(f, L, H, hlane, tab, T.ratio, rs);
-  reduce_lanes<16>(rs, hmask);
+#pragma unroll
+  for (int k = 0; k < kNumSets; ++k) rs.S[k] = 0;
+  Rounds<N, 16, 0>::run(f, tb, L, H, hlane, true, rs.S, fst);
+#pragma unroll
+  for (int off = 8; off > 0; off >>= 1) {
+#pragma unroll
+    for (int k = 0; k < kNumSets; ++k) rs.S[k] += __shfl_xor_sync(hmask, rs.S[k], off);
+  }
+  __syncwarp(hmask);
+  // fourth difference per axis (lanes 0..N-1 of the half), then the
+  // largest, the smallest axis on ties
+  rs.best = 0;
+  rs.axis = -1;
+  if (hlane < N) {
+    const double ratio = T.ratio;
+    const double base = __dmul_rn(__dmul_rn(fst[0], 2.0), __dadd_rn(1.0, -ratio));
+    const int d = hlane;
+    rs.best = fabs(__dadd_rn(__dadd_rn(base, __dmul_rn(ratio, __dadd_rn(fst[1 + 2 * d], fst[2 + 2 * d]))),
+                             -__dadd_rn(fst[1 + 2 * N + 2 * d], fst[2 + 2 * N + 2 * d])));
+    rs.axis = rs.best > 0 ? d : -1;
+  }
+#pragma unroll
+  for (int off = 8; off > 0; off >>= 1) {
+    const double ob = __shfl_xor_sync(hmask, rs.best, off);
+    const int oa = __shfl_xor_sync(hmask, rs.axis, off);
+    const bool take = (ob > rs.best) || (ob == rs.best && oa >= 0 && (rs.axis < 0 || oa < rs.axis));
+    if (take) {
+      rs.best = ob;
+      rs.axis = oa;
+    }
+  }
+  __syncwarp(hmask);  // fst is rewritten by the next evaluation
   double jac = 1;
 #pragma unroll
   for (int d = 0; d < N; ++d) jac = __dmul_rn(jac, H[d]);
@@ -216,14 +256,16 @@ __device__ __forceinline__ RegionResult eval_sub(const F& f, const double (&BL)[
 template <int N, class Src, bool kShared = false>
 __global__ void __launch_bounds__(128, kShared ? 2 : 3) k_phase2(Src src, RuleTables T,
                                                                  Phase2Args a) {
-  __shared__ detail::ItemTable<N> tab;
+  __shared__ detail::ByteTable<N> tb;
+  __shared__ double fstage[8][4 * N + 1];  // per half warp
   extern __shared__ double p2_dyn[];
-  if (threadIdx.x == 0) tab.fill();
+  tb.fill(threadIdx.x, blockDim.x);
   __syncthreads();
 
   const int lane = threadIdx.x & 31;
   const int half = lane >> 4, hlane = lane & 15;
   const unsigned hmask = half ? 0xffff0000u : 0x0000ffffu;
+  double* fst = fstage[threadIdx.x >> 4];
   const long long gwarp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / 32;
   const int stride = a.max_regions + 2;
   P2Region<N>* pool = reinterpret_cast<P2Region<N>*>(a.slab) + gwarp * stride;
@@ -260,7 +302,7 @@ __global__ void __launch_bounds__(128, kShared ? 2 : 3) k_phase2(Src src, RuleTa
     r0.div = 0;
     {
       // both halves evaluate it; half 0's result is used
-      const detail::RegionResult rr = detail::eval_sub<N>(f, BL, BW, r0, hlane, hmask, tab, T);
+      const detail::RegionResult rr = detail::eval_sub_tab<N>(f, BL, BW, r0, hlane, hmask, tb, fst, T);
       r0.avg = rr.avg;
       r0.err = rr.err;
       r0.axis = rr.axis;
@@ -292,7 +334,7 @@ __global__ void __launch_bounds__(128, kShared ? 2 : 3) k_phase2(Src src, RuleTa
           else child.lo[d] = mid;
         }
       }
-      const detail::RegionResult rr = detail::eval_sub<N>(f, BL, BW, child, hlane, hmask, tab, T);
+      const detail::RegionResult rr = detail::eval_sub_tab<N>(f, BL, BW, child, hlane, hmask, tb, fst, T);
       const double avgR = __shfl_sync(0xffffffffu, rr.avg, 16);
       const double errR0 = __shfl_sync(0xffffffffu, rr.err, 16);
       const int axR = __shfl_sync(0xffffffffu, rr.axis, 16);
