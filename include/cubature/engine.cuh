@@ -1284,7 +1284,7 @@ int run_batch(Workspace& ws, const Src& src, int nint, const double* epsrel,
       st.iterations += la.iterations;
       st.eval_launches += la.iterations;
       st.regions_evaluated += (long long)la.regions;
-      st.launches += 7ll * la.iterations;
+      st.launches += 8ll * la.iterations;  // bind, rule, partials, decide, scan, split, advance, test
       st.device_loops += 1;
       ws.peak_need = std::max(ws.peak_need, la.peak_need);
       c0.iters_done = ws.ctl_host_->iters_done;

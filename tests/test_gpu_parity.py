@@ -844,8 +844,9 @@ def test_device_loop_bit_identical(cub, ctx):
     order, so results are identical bit for bit -- a batch of 64 6-D
     product peaks whose lists outgrow the persistent kernel (breadth policy
     and the reference policy with phase-2 hand-over), a single 8-D corner
-    peak under a small persistent limit, and a breadth batch under a small
-    capacity whose loop leaves to grow the buffers."""
+    peak under a small persistent limit, a breadth batch under a small
+    capacity whose loop leaves to grow the buffers, and the 7-D table
+    integrand."""
     rng = np.random.default_rng(21)
     n = 6
     params = [cub.make_params(n, list(np.exp(rng.uniform(0, np.log(50), n))),
@@ -866,3 +867,15 @@ def test_device_loop_bit_identical(cub, ctx):
     assert ctx.stats()["device_loops"] > 0
     r2 = ctx.integrate(f, 1e-7, 1e-12, cub.options(persistent_max_n=64, device_loop=False))
     _same_bits(r1, r2, "corner peak")
+    # a table integrand (its source carries device table pointers)
+    from cubature import tables as T
+
+    tab = T.Table7(T.table7_data(0), 0)
+    offs = T.table7_offsets(3)
+    ctx.reset_stats()
+    t1 = ctx.integrate_table7_batch(tab, offs, 1e-4, 1e-12, cub.options(policy=cub.POLICY_BREADTH))
+    assert ctx.stats()["device_loops"] > 0
+    t2 = ctx.integrate_table7_batch(tab, offs, 1e-4, 1e-12,
+                                    cub.options(policy=cub.POLICY_BREADTH, device_loop=False))
+    for k, (x, y) in enumerate(zip(t1, t2)):
+        _same_bits(x, y, ("table7", k))
