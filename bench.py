@@ -718,10 +718,14 @@ def main() -> int:
         t = torch.tensor([dev_ms, wall], dtype=torch.float64, device="cuda")
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         dev_ms, wall = float(t[0]), float(t[1])
-        fb = torch.tensor([float(bad), float(bad2)], dtype=torch.float64, device="cuda")
+        # ranks may hold different numbers of integrals (balanced shares)
+        fb = torch.tensor([float(bad), float(bad2), float(nint), float(neval)],
+                          dtype=torch.float64, device="cuda")
         pg.all_reduce(fb, op=pg.ReduceOp.SUM)
-        bad, bad2 = int(fb[0]), int(fb[1])
-    good = world * nint - bad
+        bad, bad2, n_all, neval_all = int(fb[0]), int(fb[1]), int(fb[2]), int(fb[3])
+    else:
+        n_all, neval_all = nint, neval
+    good = n_all - bad
     value = good * args.steps / (dev_ms / 1e3)
     e2e_value = good * args.steps / (wall / 1e3)
 
@@ -791,7 +795,7 @@ def main() -> int:
                                  "host drives the launches); e2e: host wall clock around "
                                  "the same calls; roofline kernel times: a second pass of "
                                  "the same steps with the library's per-launch events on"},
-            "geval_per_s": world * neval * args.steps / (dev_ms / 1e3) / 1e9,
+            "geval_per_s": neval_all * args.steps / (dev_ms / 1e3) / 1e9,
             "e2e": {"value": e2e_value, "unit": "integrals/s",
                     "h2d_bytes_per_step": st.get("h2d_bytes", 0) // max(1, args.steps),
                     "d2h_bytes_per_step": st.get("d2h_bytes", 0) // max(1, args.steps)},
@@ -814,7 +818,7 @@ def main() -> int:
                          "eval_launches_per_step": st["eval_launches"] / args.steps},
             "cpu_baseline": cpu,
             "clocks": clocks.summary(),
-            "check": {"integrals": world * nint, "failed": bad, "failed_2epsrel": bad2,
+            "check": {"integrals": n_all, "failed": bad, "failed_2epsrel": bad2,
                       "rule": "status 0 and |I - I*| <= epsrel |I*| against the analytic or "
                               "closed-form I*; value and e2e count only the integrals that "
                               "pass (failed_2epsrel: the same test at 2 epsrel)"},
