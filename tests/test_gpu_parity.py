@@ -879,3 +879,25 @@ def test_device_loop_bit_identical(cub, ctx):
                                     cub.options(policy=cub.POLICY_BREADTH, device_loop=False))
     for k, (x, y) in enumerate(zip(t1, t2)):
         _same_bits(x, y, ("table7", k))
+
+
+def test_device_loop_config3_batch_bit_identical(cub, ctx):
+    """The whole 4096-integral batch of the configuration-3 generator (6-D
+    product peaks, seed = index, epsrel 1e-5, breadth policy): its
+    long-list stretches run as device-driven loops and give the host
+    loop's results bit for bit, integral by integral."""
+    n, count = 6, 4096
+    params = []
+    for k in range(count):
+        rng = np.random.default_rng(k)
+        a = np.exp(rng.uniform(np.log(1.0), np.log(50.0), n))
+        u = rng.uniform(0.1, 0.9, n)
+        params.append(cub.make_params(n, list(a), list(u)))
+    ctx.reset_stats()
+    r1 = ctx.integrate_batch("product_peak", n, params, 1e-5, 1e-12,
+                             cub.options(policy=cub.POLICY_BREADTH))
+    assert ctx.stats()["device_loops"] > 0
+    r2 = ctx.integrate_batch("product_peak", n, params, 1e-5, 1e-12,
+                             cub.options(policy=cub.POLICY_BREADTH, device_loop=False))
+    for k, (x, y) in enumerate(zip(r1, r2)):
+        _same_bits(x, y, ("config 3", k))
